@@ -1,0 +1,118 @@
+"""Loads libspotfinder_b200.so and declares its C ABI (include/spotfinder_b200.h).
+
+The library is built in-tree by ``make -C dials_metal_spotfinder_b200/csrc``
+(``__graft_entry__.build()`` runs it). There is no fallback: if the library is
+missing this module raises ImportError, and every device entry point raises
+DeviceError when no CUDA device is present.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libspotfinder_b200.so")
+HEADER_PATH = os.path.join(os.path.dirname(HERE), "include", "spotfinder_b200.h")
+
+# include/spotfinder_b200.h: sf_signal_pixel, sf_pixel, sf_spot, sf_counts.
+SIGNAL_PIXEL = np.dtype(
+    [("index", "<u4"), ("value", "<u4"), ("background", "<f4"),
+     ("population", "<u2"), ("reserved", "<u2")]
+)
+PIXEL = np.dtype([("frame", "<i4"), ("index", "<u4"), ("value", "<u4")])
+SPOT = np.dtype(
+    {
+        "names": ["bbox", "position", "variance", "intensity",
+                  "intensity_variance", "n_signal", "first"],
+        "formats": [("<i4", 6), ("<f8", 3), ("<f8", 3), "<f8", "<f8", "<u4", "<u8"],
+        "offsets": [0, 24, 48, 72, 80, 88, 96],
+        "itemsize": 104,
+    }
+)
+COUNT_NAMES = ("signal_pixels", "groups", "too_small", "too_large", "separated", "accepted")
+
+
+class BadArgument(ValueError):
+    """Status -1: the reference's 'bad argument' return."""
+
+
+class Overflow(RuntimeError):
+    """Status -2: more signal pixels than the list holds."""
+
+
+class DeviceError(RuntimeError):
+    """Status -3: a CUDA or runtime failure."""
+
+
+class Refused(RuntimeError):
+    """Status -4: a labelling input refused (order, range)."""
+
+
+class GroupOptions(ctypes.Structure):
+    _fields_ = [("min_spot_size", ctypes.c_uint64), ("max_spot_size", ctypes.c_uint64),
+                ("max_separation", ctypes.c_double), ("two_d", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+
+_P = ctypes.c_void_p
+_S = ctypes.c_size_t
+_I = ctypes.c_int
+
+# name -> (restype, argtypes). Every function the header declares appears
+# here; tests/test_abi.py checks the two lists agree and that each symbol is
+# exported.
+SIGNATURES = {
+    "sf_backend": (ctypes.c_char_p, []),
+    "sf_available": (_I, []),
+    "sf_memory_free": (_S, []),
+    "sf_host_alloc": (_P, [_S]),
+    "sf_host_free": (None, [_P]),
+    "sf_last_error": (ctypes.c_char_p, []),
+    "sf_find_u16": (_I, [_P, _S, _S, _P, _S, ctypes.POINTER(_S)]),
+    "sf_find_u32": (_I, [_P, _S, _S, _P, _S, ctypes.POINTER(_S)]),
+    "sf_profile_stages": (None, [_I]),
+    "sf_profile_stages_enabled": (_I, []),
+    "sf_last_stage_times": (None, [_P]),
+}
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is not built; run `make -C {os.path.join(HERE, 'csrc')}` "
+            "(there is no CPU fallback)"
+        )
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (restype, argtypes) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = restype
+        fn.argtypes = argtypes
+    return lib
+
+
+lib = _load()
+
+
+def last_error() -> str:
+    msg = lib.sf_last_error()
+    return msg.decode() if msg else ""
+
+
+def raise_for(status: int, what: str) -> None:
+    if status == 0:
+        return
+    if status == -1:
+        raise BadArgument(f"{what}: bad argument {last_error()}".rstrip())
+    if status == -2:
+        raise Overflow(f"{what}: more signal pixels than the list holds")
+    if status == -4:
+        raise Refused(f"{what}: {last_error()}")
+    raise DeviceError(f"{what}: {last_error() or f'status {status}'}")
+
+
+def require_device() -> None:
+    if not lib.sf_available():
+        raise DeviceError("no CUDA device is available (the B200 path has no CPU fallback)")

@@ -1,0 +1,550 @@
+// The fused extended-dispersion threshold: src/dext.cc:9-225 of the
+// reference (dispersion test, erode, masked background, Poisson test, emit),
+// as one streaming kernel per batch of frames.
+//
+// Decomposition. A task is one strip of 256 buffer columns (232 output
+// columns plus halo) by one segment of output rows of one frame. A warp owns
+// a task at a time and walks down it row by row; warps never talk to each
+// other. Each warp has a ring of 32 rows of its strip in shared memory, fed
+// 8 rows at a time by TMA (one elected lane issues, an mbarrier per stage).
+//
+// Per input row r entering at the bottom of the ring, each lane (8 columns)
+// updates, all in registers:
+//   - vertical 7-row running sums of the valid count+sum (packed) and of the
+//     sum of squares, from rows r and r-7;
+//   - the 7 x 7 window sums at row r-3 by a horizontal pass (warp shuffles
+//     for the 3 neighbour columns each side), and the dispersion test there
+//     -> one bit per pixel (masked pixels are 1, src/dext.cc:113);
+//   - the 5 x 5 erode at row r-5 on those bits (vertical AND of five
+//     8-bit rows, then horizontal AND with 2 shuffled neighbour bits);
+//   - vertical 11-row running sums of the count+sum of pixels that are valid
+//     and not kept by the erode, from rows r-5 and r-16;
+//   - at row r-10, for the rare pixels that are candidates (value > 0 and
+//     kept by the erode), the 11 x 11 window by a horizontal pass, the
+//     Poisson test, and the emit of a SignalPixel into a staging pool.
+// Every window is the reference's window clipped to the frame: the arena
+// holds the masked sentinel everywhere outside the frame, and a pixel off the
+// frame and a masked pixel are treated identically by every step of the
+// reference's arithmetic (excluded from every sum, 1 in the erode input).
+//
+// Arithmetic. Sums are exact integers; the sum of squares wraps in 32 bits
+// for 16-bit pixels (64 for 32-bit) exactly as the reference's accumulator
+// does. The two tests run in float for 16-bit pixels and double for 32-bit,
+// one IEEE rounding per operation in the reference's order, through the _rn
+// intrinsics so that nothing is contracted into an FMA.
+//
+// Output order. Records for the tile (row, strip) land contiguously in the
+// staging pool; the tile's count and start go to two small arrays. The
+// placement kernels (place.cu) then scan the counts in row-major tile order,
+// which is ascending pixel index, and copy each tile's records to the final
+// list -- so the list comes out sorted by index with no sort.
+
+#include "sf_device.cuh"
+#include "sf_host.hh"
+
+namespace sf {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr uint32_t kNoChunk = 0xffffffffu;
+
+// --------------------------------------------------------------------------
+// The two tests, in the reference's arithmetic.
+// --------------------------------------------------------------------------
+
+// src/dext.cc:97-110 with R = float.
+__device__ __forceinline__ bool dispersion(uint32_t m, uint32_t s, uint32_t q) {
+  if (m < 2)
+    return false;
+  const float mf = __uint2float_rn(m);
+  const float sf = __uint2float_rn(s);
+  const float qf = __uint2float_rn(q);
+  const float m1 = __fsub_rn(mf, 1.0f);
+  const float lhs =
+      __fsub_rn(__fsub_rn(__fmul_rn(mf, qf), __fmul_rn(sf, sf)), __fmul_rn(sf, m1));
+  const float rhs = __fmul_rn(__fmul_rn(sf, 6.0f), __fsqrt_rn(__fmul_rn(2.0f, m1)));
+  return lhs > rhs;
+}
+
+// The same with R = double, for 32-bit pixels.
+__device__ __forceinline__ bool dispersion(uint64_t m, uint64_t s, uint64_t q) {
+  if (m < 2)
+    return false;
+  const double md = __ull2double_rn(m);
+  const double sd = __ull2double_rn(s);
+  const double qd = __ull2double_rn(q);
+  const double m1 = __dsub_rn(md, 1.0);
+  const double lhs =
+      __dsub_rn(__dsub_rn(__dmul_rn(md, qd), __dmul_rn(sd, sd)), __dmul_rn(sd, m1));
+  const double rhs = __dmul_rn(__dmul_rn(sd, 6.0), __dsqrt_rn(__dmul_rn(2.0, m1)));
+  return lhs > rhs;
+}
+
+// src/dext.cc:200-213: mean over the masked window, then p >= mean + 3 sqrt(mean).
+__device__ __forceinline__ bool poisson(uint32_t p, uint32_t m, uint32_t s,
+                                        float *background) {
+  const float mean =
+      m >= 2 ? __fdiv_rn(__uint2float_rn(s), __uint2float_rn(m)) : 0.0f;
+  *background = mean;
+  return __uint2float_rn(p) >= __fadd_rn(mean, __fmul_rn(3.0f, __fsqrt_rn(mean)));
+}
+
+__device__ __forceinline__ bool poisson(uint32_t p, uint64_t m, uint64_t s,
+                                        float *background) {
+  const double mean =
+      m >= 2 ? __ddiv_rn(__ull2double_rn(s), __ull2double_rn(m)) : 0.0;
+  *background = __double2float_rn(mean);
+  return __uint2double_rn(p) >= __dadd_rn(mean, __dmul_rn(3.0, __dsqrt_rn(mean)));
+}
+
+// --------------------------------------------------------------------------
+// Row access
+// --------------------------------------------------------------------------
+
+// The lane's 8 pixels of one ring row.
+template <typename T>
+__device__ __forceinline__ void load_row(const T *row, int lane, uint32_t (&p)[8]);
+
+template <>
+__device__ __forceinline__ void load_row<uint16_t>(const uint16_t *row, int lane,
+                                                   uint32_t (&p)[8]) {
+  const uint4 v = reinterpret_cast<const uint4 *>(row)[lane];
+  p[0] = v.x & 0xffffu; p[1] = v.x >> 16;
+  p[2] = v.y & 0xffffu; p[3] = v.y >> 16;
+  p[4] = v.z & 0xffffu; p[5] = v.z >> 16;
+  p[6] = v.w & 0xffffu; p[7] = v.w >> 16;
+}
+
+template <>
+__device__ __forceinline__ void load_row<uint32_t>(const uint32_t *row, int lane,
+                                                   uint32_t (&p)[8]) {
+  const uint4 *v = reinterpret_cast<const uint4 *>(row + 8 * lane);
+  const uint4 a = v[0], b = v[1];
+  p[0] = a.x; p[1] = a.y; p[2] = a.z; p[3] = a.w;
+  p[4] = b.x; p[5] = b.y; p[6] = b.z; p[7] = b.w;
+}
+
+__device__ __forceinline__ uint32_t shfl_up(uint32_t v) { return __shfl_up_sync(kFull, v, 1); }
+__device__ __forceinline__ uint32_t shfl_down(uint32_t v) { return __shfl_down_sync(kFull, v, 1); }
+__device__ __forceinline__ uint64_t shfl_up(uint64_t v) {
+  const uint32_t lo = __shfl_up_sync(kFull, static_cast<uint32_t>(v), 1);
+  const uint32_t hi = __shfl_up_sync(kFull, static_cast<uint32_t>(v >> 32), 1);
+  return (static_cast<uint64_t>(hi) << 32) | lo;
+}
+__device__ __forceinline__ uint64_t shfl_down(uint64_t v) {
+  const uint32_t lo = __shfl_down_sync(kFull, static_cast<uint32_t>(v), 1);
+  const uint32_t hi = __shfl_down_sync(kFull, static_cast<uint32_t>(v >> 32), 1);
+  return (static_cast<uint64_t>(hi) << 32) | lo;
+}
+
+// Horizontal sums of width 2R+1 over the lane's 8 columns, given the lane's
+// own vertical sums v[0..8) and the neighbouring lanes' by shuffle. The edge
+// lanes see no neighbour; their edge columns are halo and never used.
+template <int R, typename A>
+__device__ __forceinline__ void hsum(const A (&v)[8], A (&h)[8]) {
+  A e[8 + 2 * R];
+#pragma unroll
+  for (int i = 0; i < R; i++)
+    e[i] = shfl_up(v[8 - R + i]);
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+    e[R + i] = v[i];
+#pragma unroll
+  for (int i = 0; i < R; i++)
+    e[R + 8 + i] = shfl_down(v[i]);
+  A run = 0;
+#pragma unroll
+  for (int i = 0; i < 2 * R + 1; i++)
+    run += e[i];
+  h[0] = run;
+#pragma unroll
+  for (int k = 1; k < 8; k++) {
+    run += e[k + 2 * R] - e[k - 1];
+    h[k] = run;
+  }
+}
+
+// --------------------------------------------------------------------------
+// The kernel
+// --------------------------------------------------------------------------
+
+struct ThresholdArgs {
+  const FrameDesc *frames;
+  int32_t nframes;
+  uint32_t ntasks;
+  uint32_t *tile_count; // zeroed before the launch
+  uint32_t *tile_start;
+  SignalPixel *pool;
+  uint32_t *pool_next;
+  uint32_t pool_cap; // records
+  int *status;
+  uint32_t wait_limit;
+};
+
+__device__ __forceinline__ int find_frame(const FrameDesc *frames, int n,
+                                          uint32_t task) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (frames[mid].task_begin <= task)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+template <typename T, int WPC>
+__global__ void __launch_bounds__(WPC * 32, 12 / WPC)
+    threshold_kernel(const __grid_constant__ CUtensorMap arena, ThresholdArgs args) {
+  using Tr = Traits<T>;
+  using A = typename Tr::Acc;
+  constexpr uint32_t kRowBytes = kStripCols * sizeof(T);
+  constexpr uint32_t kBoxBytes = kRowBytes * kBoxRows;
+
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  T *ring = reinterpret_cast<T *>(smem_raw + warp * (kRowBytes * kRingRows));
+  uint64_t *bars =
+      reinterpret_cast<uint64_t *>(smem_raw + WPC * (kRowBytes * kRingRows)) +
+      warp * kRingStages;
+
+  if (lane == 0) {
+    for (int s = 0; s < kRingStages; s++)
+      mbar_init(&bars[s], 1);
+    mbar_fence_init();
+  }
+  __syncwarp();
+
+  uint32_t phase = 0; // bit s = parity of the next wait on stage s
+  uint32_t chunk = kNoChunk, fill = 0;
+  bool failed = false;
+
+  const uint32_t gwarp = blockIdx.x * WPC + warp;
+  const uint32_t nwarps = gridDim.x * WPC;
+
+  for (uint32_t task = gwarp; task < args.ntasks && !failed; task += nwarps) {
+    const int f = find_frame(args.frames, args.nframes, task);
+    const FrameDesc fd = args.frames[f];
+    const uint32_t local = task - fd.task_begin;
+    const int strip = static_cast<int>(local % fd.strips);
+    const int seg = static_cast<int>(local / fd.strips);
+    const int r0 = seg * fd.seg_rows;
+    const int r1 = min(r0 + fd.seg_rows, fd.height);
+    const int rs = r0 - kHalo;       // first input row (frame coordinates)
+    const int nrows = (r1 - r0) + 2 * kHalo;
+    const int nboxes = (nrows + kBoxRows - 1) / kBoxRows;
+    const int32_t tma_x = strip * kStripOut;
+    const int64_t tma_y0 = fd.row0 + rs;
+
+    // Output columns of this lane: ring columns [10, 242) inside the frame.
+    uint32_t outmask = 0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const int j = 8 * lane + k;
+      const int col = strip * kStripOut + j - kHalo;
+      if (j >= kHalo && j < kHalo + kStripOut && col < fd.width)
+        outmask |= 1u << k;
+    }
+
+    // Prologue: the first two boxes.
+    if (lane == 0) {
+      fence_proxy_async_smem();
+      for (int b = 0; b < 2 && b < nboxes; b++) {
+        const int st = b % kRingStages;
+        mbar_expect_tx(&bars[st], kBoxBytes);
+        tma_load_2d(ring + st * kBoxRows * kStripCols, &arena, &bars[st], tma_x,
+                    static_cast<int32_t>(tma_y0 + b * kBoxRows));
+      }
+    }
+
+    A vs[8], vq[8], vg[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      vs[k] = 0; vq[k] = 0; vg[k] = 0;
+    }
+    uint64_t hist_mk = 0; // masked bits, rows r .. r-7
+    uint64_t hist_s0 = 0; // dispersion bits, rows a .. a-4 (a = r-3)
+    uint64_t gv_lo = 0;   // valid-and-not-eroded bits, rows b .. b-7 (b = r-5)
+    uint32_t gv_hi = 0;   //   rows b-8 .. b-11
+    uint64_t hist_cs = 0; // candidate-region bits, rows b .. b-5
+
+    for (int b = 0; b < nboxes && !failed; b++) {
+      const int st = b % kRingStages;
+      if (lane == 0 && b >= 1 && b + 1 < nboxes) {
+        // Box b+1 reuses the stage of box b-3, whose rows are all older than
+        // r-16 for every row of box b: free.
+        const int nst = (b + 1) % kRingStages;
+        fence_proxy_async_smem();
+        mbar_expect_tx(&bars[nst], kBoxBytes);
+        tma_load_2d(ring + nst * kBoxRows * kStripCols, &arena, &bars[nst], tma_x,
+                    static_cast<int32_t>(tma_y0 + (b + 1) * kBoxRows));
+      }
+      const bool ok = mbar_wait_bounded(&bars[st], (phase >> st) & 1u, args.wait_limit);
+      phase ^= 1u << st;
+      if (!__all_sync(kFull, ok)) {
+        if (lane == 0)
+          atomicCAS(args.status, kStatusOk, kStatusTmaTimeout);
+        failed = true;
+        break;
+      }
+
+      const int rend = min(kBoxRows, nrows - b * kBoxRows);
+      for (int i = 0; i < rend; i++) {
+        const int rr = b * kBoxRows + i;
+        const T *row_r = ring + (rr & (kRingRows - 1)) * kStripCols;
+
+        // ---- row r enters: masked bits, 7-row sums -----------------------
+        uint32_t p[8];
+        load_row<T>(row_r, lane, p);
+        uint32_t mk = 0;
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+          mk |= (p[k] >= Tr::kMasked ? 1u : 0u) << k;
+        hist_mk = (hist_mk << 8) | mk;
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          const bool valid = !((mk >> k) & 1u);
+          const A pv = valid ? static_cast<A>(p[k]) : A(0);
+          vs[k] += valid ? pv + (A(1) << Tr::kShift7) : A(0);
+          vq[k] += pv * pv;
+        }
+        if (rr >= 7) {
+          uint32_t q7[8];
+          load_row<T>(ring + ((rr - 7) & (kRingRows - 1)) * kStripCols, lane, q7);
+          const uint32_t mk7 = static_cast<uint32_t>(hist_mk >> 56) & 0xffu;
+#pragma unroll
+          for (int k = 0; k < 8; k++) {
+            const bool valid = !((mk7 >> k) & 1u);
+            const A pv = valid ? static_cast<A>(q7[k]) : A(0);
+            vs[k] -= valid ? pv + (A(1) << Tr::kShift7) : A(0);
+            vq[k] -= pv * pv;
+          }
+        }
+
+        // ---- dispersion test at row a = r-3 ------------------------------
+        if (rr >= 6) {
+          A hs[8], hq[8];
+          hsum<3>(vs, hs);
+          hsum<3>(vq, hq);
+          uint32_t s0 = static_cast<uint32_t>(hist_mk >> 24) & 0xffu; // masked -> 1
+#pragma unroll
+          for (int k = 0; k < 8; k++) {
+            const A m = hs[k] >> Tr::kShift7;
+            const A s = hs[k] & ((A(1) << Tr::kShift7) - 1);
+            s0 |= (dispersion(m, s, hq[k]) ? 1u : 0u) << k;
+          }
+          hist_s0 = (hist_s0 << 8) | s0;
+        }
+
+        // ---- erode at row b = r-5, and the 11-row sums -------------------
+        if (rr >= 10) {
+          const uint32_t v = static_cast<uint32_t>(hist_s0 & (hist_s0 >> 8) &
+                                                   (hist_s0 >> 16) & (hist_s0 >> 24) &
+                                                   (hist_s0 >> 32)) & 0xffu;
+          const uint32_t vl = shfl_up(v), vr = shfl_down(v);
+          const uint32_t w = (vl >> 6) | (v << 2) | (vr << 10);
+          const uint32_t hv = w & (w >> 1) & (w >> 2) & (w >> 3) & (w >> 4) & 0xffu;
+          const uint32_t mkb = static_cast<uint32_t>(hist_mk >> 40) & 0xffu;
+          const uint32_t s1 = hv | mkb;           // scr1, src/dext.cc:117-142
+          const uint32_t gv = ~s1 & 0xffu;        // valid and not kept
+          const uint32_t cs = s1 & ~mkb & 0xffu;  // kept and not masked
+          gv_hi = (gv_hi << 8) | static_cast<uint32_t>(gv_lo >> 56);
+          gv_lo = (gv_lo << 8) | gv;
+          hist_cs = (hist_cs << 8) | cs;
+
+          uint32_t p5[8];
+          load_row<T>(ring + ((rr - 5) & (kRingRows - 1)) * kStripCols, lane, p5);
+#pragma unroll
+          for (int k = 0; k < 8; k++)
+            vg[k] += ((gv >> k) & 1u) ? static_cast<A>(p5[k]) + (A(1) << Tr::kShift11) : A(0);
+
+          if (rr >= 21) {
+            const uint32_t gv16 = (gv_hi >> 24) & 0xffu;
+            uint32_t p16[8];
+            load_row<T>(ring + ((rr - 16) & (kRingRows - 1)) * kStripCols, lane, p16);
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+              vg[k] -= ((gv16 >> k) & 1u) ? static_cast<A>(p16[k]) + (A(1) << Tr::kShift11)
+                                          : A(0);
+          }
+        }
+
+        // ---- Poisson test and emit at row c = r-10 -----------------------
+        if (rr >= 2 * kHalo) {
+          const int c = rs + rr - kHalo; // frame row of the output
+          const uint32_t cs = static_cast<uint32_t>(hist_cs >> 40) & 0xffu & outmask;
+          if (__any_sync(kFull, cs != 0)) {
+            A hg[8];
+            hsum<5>(vg, hg);
+            uint32_t pc[8];
+            load_row<T>(ring + ((rr - kHalo) & (kRingRows - 1)) * kStripCols, lane, pc);
+            uint32_t sig = 0;
+            float bg[8];
+            uint32_t pop[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+              bg[k] = 0.0f;
+              pop[k] = static_cast<uint32_t>(hg[k] >> Tr::kShift11);
+              if (((cs >> k) & 1u) && pc[k] > 0) {
+                const A m = hg[k] >> Tr::kShift11;
+                const A s = hg[k] & ((A(1) << Tr::kShift11) - 1);
+                if (poisson(pc[k], m, s, &bg[k]))
+                  sig |= 1u << k;
+              }
+            }
+            const uint32_t cnt = __popc(sig);
+            uint32_t incl = cnt;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+              const uint32_t t = __shfl_up_sync(kFull, incl, d);
+              if (lane >= d)
+                incl += t;
+            }
+            const uint32_t total = __shfl_sync(kFull, incl, 31);
+            if (total > 0) {
+              if (chunk == kNoChunk || fill + total > kChunkRecords) {
+                uint32_t base = 0;
+                if (lane == 0)
+                  base = atomicAdd(args.pool_next, kChunkRecords);
+                base = __shfl_sync(kFull, base, 0);
+                if (base > args.pool_cap - kChunkRecords || base + kChunkRecords < base) {
+                  if (lane == 0)
+                    atomicCAS(args.status, kStatusOk, kStatusPoolExhausted);
+                  chunk = kNoChunk;
+                } else {
+                  chunk = base;
+                }
+                fill = 0;
+              }
+              const uint64_t tile = fd.tile_base + static_cast<uint64_t>(c) * fd.strips + strip;
+              if (chunk != kNoChunk) {
+                const uint32_t start = chunk + fill;
+                fill += total;
+                uint32_t at = start + (incl - cnt);
+                const uint32_t col0 = strip * kStripOut + 8 * lane - kHalo;
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                  if ((sig >> k) & 1u) {
+                    SignalPixel px;
+                    px.index = static_cast<uint32_t>(c) * static_cast<uint32_t>(fd.width) + col0 + k;
+                    px.value = pc[k];
+                    px.background = bg[k];
+                    px.population = static_cast<uint16_t>(pop[k]);
+                    px.reserved = 0;
+                    args.pool[at++] = px;
+                  }
+                }
+                if (lane == 0) {
+                  args.tile_count[tile] = total;
+                  args.tile_start[tile] = start;
+                }
+              } else if (lane == 0) {
+                args.tile_count[tile] = total; // counted, records dropped
+                args.tile_start[tile] = 0;
+              }
+            }
+          }
+        }
+      }
+      __syncwarp();
+    }
+    if (failed) {
+      // Let any copy still in flight land before this warp's shared memory
+      // is released; bounded, like every wait here.
+      for (int s = 0; s < kRingStages; s++)
+        mbar_wait_bounded(&bars[s], (phase >> s) & 1u, args.wait_limit);
+    }
+  }
+}
+
+} // namespace
+
+// --------------------------------------------------------------------------
+// Host side
+// --------------------------------------------------------------------------
+
+template <typename T>
+size_t threshold_smem_bytes(int wpc) {
+  return static_cast<size_t>(wpc) * (kStripCols * sizeof(T) * kRingRows) +
+         static_cast<size_t>(wpc) * kRingStages * sizeof(uint64_t);
+}
+
+template <typename T, int WPC>
+static cudaError_t launch_wpc(const CUtensorMap &map, const ThresholdLaunch &L,
+                              cudaStream_t stream) {
+  const size_t smem = threshold_smem_bytes<T>(WPC);
+  static bool configured = false; // per instantiation; setting it twice is harmless
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(threshold_kernel<T, WPC>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess)
+      return e;
+    configured = true;
+  }
+  ThresholdArgs a;
+  a.frames = L.frames;
+  a.nframes = L.nframes;
+  a.ntasks = L.ntasks;
+  a.tile_count = L.tile_count;
+  a.tile_start = L.tile_start;
+  a.pool = L.pool;
+  a.pool_next = L.pool_next;
+  a.pool_cap = L.pool_cap;
+  a.status = L.status;
+  a.wait_limit = L.wait_limit;
+  const uint32_t warps_needed = L.ntasks;
+  uint32_t blocks = (warps_needed + WPC - 1) / WPC;
+  if (L.max_blocks > 0 && blocks > static_cast<uint32_t>(L.max_blocks))
+    blocks = static_cast<uint32_t>(L.max_blocks);
+  if (blocks == 0)
+    return cudaSuccess;
+  threshold_kernel<T, WPC><<<blocks, WPC * 32, smem, stream>>>(map, a);
+  return cudaGetLastError();
+}
+
+template <typename T, int WPC> static int occupancy_wpc() {
+  const size_t smem = threshold_smem_bytes<T>(WPC);
+  if (cudaFuncSetAttribute(threshold_kernel<T, WPC>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(smem)) != cudaSuccess)
+    return 0;
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, threshold_kernel<T, WPC>, WPC * 32,
+                                                    smem) != cudaSuccess)
+    return 0;
+  return n;
+}
+
+template <typename T> int threshold_occupancy(int wpc) {
+  switch (wpc) {
+  case 1: return occupancy_wpc<T, 1>();
+  case 2: return occupancy_wpc<T, 2>();
+  case 4: return occupancy_wpc<T, 4>();
+  default: return 0;
+  }
+}
+
+template <typename T>
+cudaError_t launch_threshold(const CUtensorMap &map, const ThresholdLaunch &L,
+                             cudaStream_t stream) {
+  switch (L.warps_per_block) {
+  case 1: return launch_wpc<T, 1>(map, L, stream);
+  case 2: return launch_wpc<T, 2>(map, L, stream);
+  case 4: return launch_wpc<T, 4>(map, L, stream);
+  default: return cudaErrorInvalidValue;
+  }
+}
+
+template cudaError_t launch_threshold<uint16_t>(const CUtensorMap &, const ThresholdLaunch &,
+                                                cudaStream_t);
+template cudaError_t launch_threshold<uint32_t>(const CUtensorMap &, const ThresholdLaunch &,
+                                                cudaStream_t);
+template size_t threshold_smem_bytes<uint16_t>(int);
+template int threshold_occupancy<uint16_t>(int);
+template int threshold_occupancy<uint32_t>(int);
+template size_t threshold_smem_bytes<uint32_t>(int);
+
+} // namespace sf
