@@ -1,0 +1,438 @@
+#!/usr/bin/env python3
+"""Benchmark of the spot-finder hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--batch F] [--pool P]
+
+Workload: Eiger2-16M-shaped uint16 frames (4362 x 4148, slow x fast), seeded
+synthetic data with module gaps, a Poisson ring background and 6000 Gaussian
+reflections per frame. One step is one batch of F frames (default 16) through
+the batched engine: the fused threshold kernel and the ordered compaction,
+frames resident in HBM, two slots of distinct frames alternating. Every batch
+is 580 MB, well over the 126 MB L2, so each step re-reads its frames from HBM.
+
+Prints one JSON line (rank 0). `value` is frames/s over the timed steps from
+CUDA events on the engine's stream (max over ranks); `e2e` is the same metric
+through the public API from pinned host frames, with the host-to-device copy
+of the frames and the device-to-host read of the signal lists inside the
+timed region; `roofline` is the threshold kernel's algorithmic bytes per
+launch over its event-timed launch duration; `cpu_baseline` is the
+reference's own CPU code (dext.cc + dials_spots.cc, compiled from the
+reference sources) on a bounded sample, all host cores.
+
+--impl reference times that reference CPU path alone as the bench's reference
+arm, on the same workload, metric and unit.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "16M uint16 frames/s (threshold+3D label), % HBM roofline; p99 frame latency"
+UNIT = "frames/s"
+SHAPE = (4362, 4148)
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--pool", type=int, default=8, help="distinct synthetic frames")
+    ap.add_argument("--e2e-steps", type=int, default=4)
+    ap.add_argument("--cpu-frames", type=int, default=8)
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# -- ranks ------------------------------------------------------------------
+
+class Ranks:
+    """One process per GPU under torchrun; replicas only (no data exchange on
+    the path), so the process group carries nothing but barriers and the
+    max-over-ranks of the timings."""
+
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+            self.dist = dist
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, v: float) -> float:
+        if self.world == 1:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, v: float) -> float:
+        if self.world == 1:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
+
+
+# -- clocks -----------------------------------------------------------------
+
+REASONS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap",
+           0x8: "hw_slowdown", 0x10: "sync_boost", 0x20: "sw_thermal_slowdown",
+           0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown",
+           0x100: "display_clock_setting"}
+
+
+class ClockSampler:
+    def __init__(self, device: int):
+        self.device = device
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 4:
+                try:
+                    self.samples.append((float(parts[0]), float(parts[1]),
+                                         float(parts[2]), int(parts[3], 16)))
+                except ValueError:
+                    pass
+
+    def __exit__(self, *exc):
+        time.sleep(0.3)
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        busy = [s for s in self.samples if not (s[3] & 0x1)] or self.samples
+        mask = 0
+        for s in busy:
+            mask |= s[3]
+        return {"sm_mhz": statistics.median(s[0] for s in busy),
+                "sm_max_mhz": max(s[1] for s in busy),
+                "power_w_max": max(s[2] for s in busy),
+                "samples": len(busy),
+                "reasons": [name for bit, name in REASONS.items() if mask & bit and bit != 0x1]}
+
+
+# -- data -------------------------------------------------------------------
+
+def make_pool(n: int):
+    from dials_metal_spotfinder_b200 import synth
+    series = synth.eiger_16m(frames=max(n, 3))
+    return [series.frame(f) for f in range(n)]
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def recorded_traffic():
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
+            return json.load(fh)
+    except (OSError, ValueError):
+        return {}
+
+
+# -- the reference CPU path -------------------------------------------------
+
+def cpu_reference(frames, threads):
+    """The reference's dext<uint16_t> on `threads` workers over frames already
+    in memory, and its Labeller fed in frame order on this thread, as
+    src/find_spots.cc:472-591 does without the HDF5 read and decompression.
+    Uses oracle/_ref (the reference's own sources) where built, else the C
+    restatement. Returns (seconds, kind)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle import oracle as O
+    use_ref = O.ref_available()
+    h, w = frames[0].shape
+    t0 = time.perf_counter()
+    lab = O.Labeller(h, w, use_ref=use_ref)
+    with ThreadPoolExecutor(threads) as pool:
+        for z, (status, sig, _) in enumerate(pool.map(lambda im: O.dext(im, use_ref=use_ref),
+                                                      frames)):
+            lab.add(z, sig)
+    lab.finish()
+    return time.perf_counter() - t0, ("reference" if use_ref else "port")
+
+
+# -- arms -------------------------------------------------------------------
+
+def run_reference_arm(args, ranks):
+    if ranks.rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    n = max(2, args.cpu_frames)
+    frames = make_pool(n)
+    for _ in range(max(0, min(args.warmup, 1))):
+        cpu_reference(frames[:2], threads)
+    times = []
+    for _ in range(max(1, args.steps)):
+        dt, kind = cpu_reference(frames, threads)
+        times.append(dt)
+        if sum(times) > 120:
+            break
+    value = n * len(times) / sum(times)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": len(times), "warmup": args.warmup,
+        "ms_per_step": 1000 * sum(times) / len(times), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u16/f32", "data": "synthetic",
+        "config": {"workload": "16M uint16 frames, threshold + 3D grouping on the host",
+                   "frames_per_step": n, "shape": list(SHAPE)},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": f"{n} frames of 4362x4148 per step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_ours(args, ranks):
+    import dials_metal_spotfinder_b200 as sf
+    from dials_metal_spotfinder_b200 import _lib
+    from dials_metal_spotfinder_b200.engine import Engine
+
+    _lib.raise_for(_lib.lib.sf_set_device(ranks.local), "sf_set_device")
+    F = args.batch
+    pool = make_pool(args.pool)
+    frame_bytes = SHAPE[0] * SHAPE[1] * 2
+    eng = Engine([SHAPE] * F, np.uint16, slots=2)
+    info = eng.info()
+    for s in range(2):
+        for f in range(F):
+            eng.upload(s, f, pool[(s * F + f) % len(pool)])
+    eng.synchronize()
+
+    # warm-up
+    for i in range(args.warmup):
+        eng.run(i % 2)
+    eng.synchronize()
+
+    # timed: resident frames
+    eng.profile(True)
+    ranks.barrier()
+    with ClockSampler(ranks.local) as clocks:
+        eng.record(0)
+        for i in range(args.steps):
+            eng.run(i % 2)
+        eng.record(1)
+        eng.synchronize()
+    ms = eng.elapsed_ms(0, 1)
+    ranks.barrier()
+    ms_max = ranks.max(ms)
+    stage = eng.stage_totals()
+    eng.profile(False)
+    counts = [eng.counts(s) for s in range(2)]
+    nsig_per_step = [int(c.sum()) for c in counts]
+    frames_total = ranks.sum(F * args.steps)
+    value = frames_total / (ms_max / 1000.0)
+
+    # roofline of the threshold kernel: algorithmic bytes per launch (one read
+    # of every frame plus one 16-byte record per signal pixel) over the
+    # kernel's average event-timed duration
+    alg_bytes = statistics.mean(F * frame_bytes + 16 * n for n in nsig_per_step)
+    thr_ms = stage["threshold_ms"] / max(stage["runs"], 1)
+    achieved = alg_bytes / (thr_ms / 1000.0) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = recorded_traffic().get(f"threshold_u16_{SHAPE[0]}x{SHAPE[1]}_per_frame")
+
+    # e2e: pinned host frames -> device -> signal lists back, per step
+    e2e = None
+    if args.e2e_steps > 0:
+        hb = [sf.HostBuffer(SHAPE, np.uint16) for _ in range(F)]
+        for f in range(F):
+            hb[f].array[:] = pool[f % len(pool)]
+        sig_buf = np.empty(frame_bytes // 16, sf.SIGNAL_PIXEL)
+        d2h = 0
+
+        def e2e_step(slot):
+            nonlocal d2h
+            for f in range(F):
+                eng.upload(slot, f, hb[f].array)
+            eng.run(slot)
+            c = eng.counts(slot)
+            for f in range(F):
+                import ctypes
+                found = ctypes.c_size_t(0)
+                _lib.raise_for(_lib.lib.sf_engine_signal(eng._h, slot, f, sig_buf.ctypes.data,
+                                                         len(sig_buf), ctypes.byref(found)),
+                               "signal")
+            d2h = int(c.sum()) * 16 + 4 * F
+        e2e_step(0)
+        eng.synchronize()
+        ranks.barrier()
+        t0 = time.perf_counter()
+        for i in range(args.e2e_steps):
+            e2e_step(i % 2)
+        eng.synchronize()
+        dt = ranks.max(time.perf_counter() - t0)
+        e2e = {"value": ranks.sum(F * args.e2e_steps) / dt, "unit": UNIT,
+               "h2d_bytes_per_step": F * frame_bytes, "d2h_bytes_per_step": d2h,
+               "timer": "host wall clock, synchronised at both ends"}
+        for b in hb:
+            b.close()
+
+    # the plain per-frame GPU form, the same frame through sf_find_u16
+    plain = None
+    if ranks.rank == 0:
+        hb0 = sf.HostBuffer(SHAPE, np.uint16)
+        hb0.array[:] = pool[0]
+        for _ in range(2):
+            sf.find(hb0.array)
+        t0 = time.perf_counter()
+        nplain = 10
+        for _ in range(nplain):
+            sf.find(hb0.array)
+        plain = {"value": nplain / (time.perf_counter() - t0), "unit": UNIT,
+                 "form": "sf_find_u16, one frame per call from pinned host memory"}
+        hb0.close()
+
+    ref_gpu = None
+    if ranks.rank == 0:
+        ref_gpu = reference_gpu_form(pool[0])
+
+    cpu = None
+    if ranks.rank == 0 and ranks.world == 1 and not args.no_cpu:
+        n = max(2, args.cpu_frames)
+        frames = [pool[i % len(pool)] for i in range(n)]
+        threads = os.cpu_count() or 1
+        dt, kind = cpu_reference(frames, threads)
+        cpu = {"value": n / dt, "unit": UNIT, "cores": threads, "kind": kind,
+               "sample": f"{n} frames of 4362x4148, threshold on {threads} threads "
+                         "and 3D grouping on one, as the reference CLI runs them"}
+
+    launches_per_step = 4  # threshold + placement reduce, scan, copy
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ranks.world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u16 pixels, u32 sums, f32 tests", "data": "synthetic",
+        "config": {"workload": "Eiger2-16M-shaped uint16 frames, 4362x4148, batched engine",
+                   "frames_per_step": F, "slots": 2, "distinct_frames": len(pool),
+                   "pipeline": "threshold + ordered compaction (grouping not yet in the timed step)",
+                   "l2": "inputs larger than L2 (580 MB per step)",
+                   "parallelism": f"replicas x{ranks.world}",
+                   "engine": info},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "kernel": "threshold_kernel<uint16_t>",
+                     "kernel_ms_per_launch": thr_ms,
+                     "algorithmic_bytes_per_launch": alg_bytes,
+                     "traffic": (traffic * F if traffic else None)},
+        "stage_ms_per_step": {"threshold": thr_ms,
+                              "placement": stage["place_ms"] / max(stage["runs"], 1)},
+        "signal_pixels_per_frame": statistics.mean(nsig_per_step) / F,
+        "clocks": clocks.summary(),
+        "gpu_launches": launches_per_step * args.steps,
+        "e2e": e2e,
+        "plain_gpu": plain,
+        "reference_gpu": ref_gpu,
+        "cpu_baseline": cpu,
+    }
+    eng.close()
+    if ranks.rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def reference_gpu_form(frame):
+    """The reference's own CUDA backend (src/dext_cuda.cu via its gpu::find),
+    built for sm_100a from the reference sources, on the same frame."""
+    try:
+        import ctypes
+
+        from oracle import oracle as O
+        lib = O.ref_gpu_lib()
+    except Exception as exc:  # not built where the reference tree was absent
+        return {"unavailable": str(exc)}
+    import dials_metal_spotfinder_b200 as sf
+    lib.refgpu_quiet()
+    hb = sf.HostBuffer(frame.shape, np.uint16)
+    hb.array[:] = frame
+    cap = frame.size * 2 // 16
+    out = np.empty(cap, sf.SIGNAL_PIXEL)
+    found = ctypes.c_size_t(0)
+    for _ in range(2):
+        lib.refgpu_find_u16(hb.array.ctypes.data, frame.shape[0], frame.shape[1],
+                            out.ctypes.data, cap, ctypes.byref(found))
+    n = 10
+    t0 = time.perf_counter()
+    for _ in range(n):
+        st = lib.refgpu_find_u16(hb.array.ctypes.data, frame.shape[0], frame.shape[1],
+                                 out.ctypes.data, cap, ctypes.byref(found))
+    dt = time.perf_counter() - t0
+    hb.close()
+    return {"value": n / dt, "unit": UNIT, "status": st, "signal_pixels": found.value,
+            "form": "reference src/dext_cuda.cu gpu::find, one frame per call, sm_100a"}
+
+
+def main():
+    args = parse()
+    ranks = Ranks()
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, ranks)
+        else:
+            run_ours(args, ranks)
+    finally:
+        ranks.close()
+
+
+if __name__ == "__main__":
+    main()

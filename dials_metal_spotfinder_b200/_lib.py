@@ -71,12 +71,32 @@ SIGNATURES = {
     "sf_host_alloc": (_P, [_S]),
     "sf_host_free": (None, [_P]),
     "sf_last_error": (ctypes.c_char_p, []),
+    "sf_set_device": (_I, [_I]),
     "sf_find_u16": (_I, [_P, _S, _S, _P, _S, ctypes.POINTER(_S)]),
     "sf_find_u32": (_I, [_P, _S, _S, _P, _S, ctypes.POINTER(_S)]),
     "sf_profile_stages": (None, [_I]),
     "sf_profile_stages_enabled": (_I, []),
     "sf_last_stage_times": (None, [_P]),
+    "sf_engine_create": (_I, [_I, _I, _P, _P, _P, ctypes.POINTER(_P)]),
+    "sf_engine_destroy": (None, [_P]),
+    "sf_engine_info": (_I, [_P, _P]),
+    "sf_engine_upload": (_I, [_P, _I, _I, _P]),
+    "sf_engine_upload_device": (_I, [_P, _I, _I, _P, _S]),
+    "sf_engine_run": (_I, [_P, _I]),
+    "sf_engine_use_graph": (_I, [_P, _I]),
+    "sf_engine_synchronize": (_I, [_P]),
+    "sf_engine_counts": (_I, [_P, _I, _P]),
+    "sf_engine_signal": (_I, [_P, _I, _I, _P, _S, ctypes.POINTER(_S)]),
+    "sf_engine_record": (_I, [_P, _I]),
+    "sf_engine_elapsed": (_I, [_P, _I, _I, ctypes.POINTER(ctypes.c_float)]),
+    "sf_engine_profile": (_I, [_P, _I]),
+    "sf_engine_stage_totals": (_I, [_P, _P]),
 }
+
+
+class EngineConfig(ctypes.Structure):
+    _fields_ = [("seg_rows", ctypes.c_int32), ("warps_per_block", ctypes.c_int32),
+                ("blocks_per_sm", ctypes.c_int32), ("slots", ctypes.c_int32)]
 
 
 def _load():

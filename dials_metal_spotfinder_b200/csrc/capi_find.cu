@@ -13,6 +13,7 @@
 #include <memory>
 
 #include "../../include/spotfinder_b200.h"
+#include "sf_capi.hh"
 #include "sf_host.hh"
 
 namespace sf {
@@ -72,10 +73,9 @@ struct FindWorkspace {
     plan.reset();
     std::vector<ThresholdPlan::Shape> shapes{
         {static_cast<int32_t>(height), static_cast<int32_t>(width)}};
-    // One frame per launch: short segments so a single frame still spreads
-    // over every SM.
-    const int seg = height >= 2048 ? 128 : 64;
-    plan = std::make_unique<ThresholdPlan>(elem_bytes, shapes, seg, 4, 0);
+    // One frame per launch: the plan picks segments short enough that a
+    // single frame still spreads over every SM.
+    plan = std::make_unique<ThresholdPlan>(elem_bytes, shapes, PlanTuning{}, 1);
     eb = elem_bytes;
     h = height;
     w = width;
@@ -112,17 +112,16 @@ int find_impl(int elem_bytes, const void *image, size_t height, size_t width,
 
   if (timing)
     check(cudaEventRecord(ev[0], s), "cudaEventRecord");
-  plan.upload(0, image, s);
+  plan.upload(0, 0, image, s);
   if (timing)
     check(cudaEventRecord(ev[1], s), "cudaEventRecord");
-  plan.enqueue(s);
+  plan.enqueue(0, s, timing ? ev[2] : nullptr);
   if (timing)
     check(cudaEventRecord(ev[3], s), "cudaEventRecord");
-  check(cudaMemcpyAsync(ws.pinned, plan.frame_count(), sizeof(uint32_t),
+  // The count and the status word are adjacent: one copy.
+  check(cudaMemcpyAsync(ws.pinned, plan.frame_count(0), 2 * sizeof(uint32_t),
                         cudaMemcpyDeviceToHost, s),
         "reading the signal count back");
-  check(cudaMemcpyAsync(ws.pinned + 1, plan.status(), sizeof(int), cudaMemcpyDeviceToHost, s),
-        "reading the status back");
   check(cudaStreamSynchronize(s), "cudaStreamSynchronize");
 
   const uint32_t count = ws.pinned[0];
@@ -134,10 +133,11 @@ int find_impl(int elem_bytes, const void *image, size_t height, size_t width,
     float ms = 0;
     check(cudaEventElapsedTime(&ms, ev[0], ev[1]), "upload time");
     g_times[0] = ms;
-    check(cudaEventElapsedTime(&ms, ev[1], ev[3]), "threshold time");
-    g_times[1] = ms; // threshold and placement together unless split below
+    check(cudaEventElapsedTime(&ms, ev[1], ev[2]), "threshold time");
+    g_times[1] = ms;
     g_times[2] = 0;
-    g_times[3] = 0;
+    check(cudaEventElapsedTime(&ms, ev[2], ev[3]), "placement time");
+    g_times[3] = ms;
     g_times[4] = 0;
     g_times[5] = 0;
   }
@@ -146,7 +146,7 @@ int find_impl(int elem_bytes, const void *image, size_t height, size_t width,
   if (count == 0)
     return 0;
   const auto t0 = std::chrono::steady_clock::now();
-  check(cudaMemcpyAsync(out, plan.out() + plan.out_base(0), count * sizeof(SignalPixel),
+  check(cudaMemcpyAsync(out, plan.out(0) + plan.out_base(0), count * sizeof(SignalPixel),
                         cudaMemcpyDeviceToHost, s),
         "copying the signal pixels back");
   check(cudaStreamSynchronize(s), "cudaStreamSynchronize");
@@ -155,21 +155,6 @@ int find_impl(int elem_bytes, const void *image, size_t height, size_t width,
         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
             .count();
   return 0;
-}
-
-template <typename F> int guarded(F &&body) {
-  try {
-    return body();
-  } catch (const DeviceError &e) {
-    set_error(e.what());
-    return -3;
-  } catch (const std::invalid_argument &e) {
-    set_error(e.what());
-    return -1;
-  } catch (const std::exception &e) {
-    set_error(e.what());
-    return -3;
-  }
 }
 
 } // namespace
@@ -206,6 +191,13 @@ void sf_host_free(void *pointer) {
 }
 
 const char *sf_last_error(void) { return sf::g_last_error.c_str(); }
+
+int sf_set_device(int device) {
+  return guarded([&] {
+    sf::check(cudaSetDevice(device), "cudaSetDevice");
+    return 0;
+  });
+}
 
 int sf_find_u16(const uint16_t *image, size_t height, size_t width, sf_signal_pixel *out,
                 size_t capacity, size_t *found) {

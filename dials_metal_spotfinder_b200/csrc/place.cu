@@ -8,8 +8,10 @@
 //   place_reduce  per-block sums of kPlaceTiles tile counts
 //   place_scan    one block: exclusive scan of the block sums, and each
 //                 frame's starting offset and signal count
-//   place_copy    per-block scan of its tiles, then a copy of every non-empty
-//                 tile's records to their final position
+//   place_copy    per-block scan of its tiles, then a record-parallel copy:
+//                 the block's records are one contiguous run of the output
+//                 (within a frame), so thread k copies record k after a
+//                 binary search for its tile in shared memory
 
 #include "sf_host.hh"
 
@@ -128,7 +130,10 @@ __global__ void __launch_bounds__(kPlaceThreads)
                const uint32_t *block_sums, const FrameDesc *frames, int nframes,
                const uint32_t *frame_prefix, const SignalPixel *pool,
                SignalPixel *out) {
-  __shared__ uint32_t offs[kPlaceTiles];
+  __shared__ uint32_t off[kPlaceTiles]; // exclusive prefix of counts within the block
+  __shared__ uint32_t src[kPlaceTiles]; // pool index of the tile's first record
+  __shared__ uint32_t dst[kPlaceTiles]; // output index of the tile's first record
+  __shared__ uint32_t lim[kPlaceTiles]; // records of the tile that fit its frame's list
   const uint64_t block_base = static_cast<uint64_t>(blockIdx.x) * kPlaceTiles;
   const uint64_t base = block_base + static_cast<uint64_t>(threadIdx.x) * kPlaceItems;
   uint32_t c[kPlaceItems];
@@ -139,38 +144,41 @@ __global__ void __launch_bounds__(kPlaceThreads)
     sum += c[i];
   }
   uint32_t total;
-  uint32_t run = block_excl_scan(sum, &total) + block_sums[blockIdx.x];
+  uint32_t run = block_excl_scan(sum, &total);
+  const uint32_t block_prefix = block_sums[blockIdx.x];
 #pragma unroll
   for (int i = 0; i < kPlaceItems; i++) {
-    offs[threadIdx.x * kPlaceItems + i] = run;
+    const int t = threadIdx.x * kPlaceItems + i;
+    off[t] = run;
+    if (c[i] != 0) {
+      const uint64_t tile = base + i;
+      const int f = frame_of_tile(frames, nframes, tile);
+      const uint32_t at = block_prefix + run - frame_prefix[f]; // position in frame f's list
+      const uint32_t cap = frames[f].capacity;
+      src[t] = starts[tile];
+      dst[t] = static_cast<uint32_t>(frames[f].out_base) + at;
+      lim[t] = at >= cap ? 0u : min(c[i], cap - at);
+    } else {
+      lim[t] = 0;
+    }
     run += c[i];
   }
   __syncthreads();
-  if (total == 0)
-    return;
 
-  // Warps walk the block's tiles 32 at a time and copy the non-empty ones.
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int t0 = warp * 32; t0 < kPlaceTiles; t0 += kPlaceThreads) {
-    const uint64_t tile = block_base + t0 + lane;
-    const uint32_t n = tile < ntiles ? counts[tile] : 0u;
-    uint32_t pending = __ballot_sync(kFull, n != 0);
-    while (pending) {
-      const int src_lane = __ffs(pending) - 1;
-      pending &= pending - 1;
-      const uint64_t t = block_base + t0 + src_lane;
-      const uint32_t cnt = __shfl_sync(kFull, n, src_lane);
-      const int f = frame_of_tile(frames, nframes, t);
-      const uint32_t at = offs[t0 + src_lane] - frame_prefix[f];
-      const uint32_t cap = frames[f].capacity;
-      const uint32_t start = starts[t];
-      SignalPixel *dst = out + frames[f].out_base;
-      for (uint32_t k = lane; k < cnt; k += 32) {
-        if (at + k < cap) {
-          const uint4 v = reinterpret_cast<const uint4 *>(pool)[start + k];
-          reinterpret_cast<uint4 *>(dst)[at + k] = v;
-        }
-      }
+  for (uint32_t k = threadIdx.x; k < total; k += kPlaceThreads) {
+    // The tile holding record k: the last t with off[t] <= k.
+    int lo = 0, hi = kPlaceTiles - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (off[mid] <= k)
+        lo = mid;
+      else
+        hi = mid - 1;
+    }
+    const uint32_t j = k - off[lo];
+    if (j < lim[lo]) {
+      const uint4 v = reinterpret_cast<const uint4 *>(pool)[src[lo] + j];
+      reinterpret_cast<uint4 *>(out)[dst[lo] + j] = v;
     }
   }
 }

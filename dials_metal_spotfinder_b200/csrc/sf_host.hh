@@ -27,6 +27,8 @@ inline void check(cudaError_t status, const char *what) {
     throw DeviceError(std::string("CUDA: ") + what + ": " + cudaGetErrorString(status));
 }
 
+void set_error(const char *what);
+
 struct ThresholdLaunch {
   const FrameDesc *frames;
   int32_t nframes;
@@ -46,6 +48,7 @@ template <typename T>
 cudaError_t launch_threshold(const CUtensorMap &map, const ThresholdLaunch &L,
                              cudaStream_t stream);
 template <typename T> size_t threshold_smem_bytes(int wpc);
+template <typename T> int threshold_occupancy(int wpc);
 
 // Ordered compaction of the staged records (place.cu).
 struct PlaceLaunch {
@@ -61,7 +64,7 @@ struct PlaceLaunch {
   uint32_t *frame_count;  // nframes
 };
 constexpr int kPlaceThreads = 256;
-constexpr int kPlaceItems = 16;
+constexpr int kPlaceItems = 4;
 constexpr int kPlaceTiles = kPlaceThreads * kPlaceItems;
 
 cudaError_t launch_place(const PlaceLaunch &L, cudaStream_t stream);
@@ -73,10 +76,18 @@ void encode_arena_map(CUtensorMap *map, void *base, int elem_bytes,
 
 int device_sm_count();
 
-// The device buffers for thresholding one batch shape: the arena the frames
-// are copied into, the tile arrays, the staging pool and the output lists.
-// Built once per shape and reused; every launch it enqueues is capturable in
-// a CUDA graph.
+// Launch geometry of the threshold for one batch shape.
+struct PlanTuning {
+  int seg_rows = 0;        // output rows per task; 0 picks by frame count
+  int warps_per_block = 4; // 1, 2 or 4
+  int blocks_per_sm = 0;   // 0: as many as fit
+};
+
+// The device buffers for thresholding one batch shape: `slots` arenas the
+// frames are copied into (each with its own TMA descriptor and output lists,
+// so one slot can be filled or read while another is computed), and the tile
+// arrays and staging pool the runs share. Built once per shape and reused;
+// every launch it enqueues is capturable in a CUDA graph.
 class ThresholdPlan {
 public:
   struct Shape {
@@ -84,65 +95,73 @@ public:
     int32_t width;
   };
 
-  ThresholdPlan(int elem_bytes, const std::vector<Shape> &shapes, int seg_rows,
-                int warps_per_block, int blocks_per_sm);
+  ThresholdPlan(int elem_bytes, const std::vector<Shape> &shapes, const PlanTuning &tuning,
+                int slots = 1);
   ~ThresholdPlan();
   ThresholdPlan(const ThresholdPlan &) = delete;
   ThresholdPlan &operator=(const ThresholdPlan &) = delete;
 
-  // Enqueue the threshold and the placement on `stream`. Frames must already
-  // be in the arena.
-  void enqueue(cudaStream_t stream);
+  // Enqueue the threshold of slot `slot` on `stream`: clears, threshold,
+  // placement. When `mid` is given it is recorded between the threshold and
+  // the placement, so the two can be timed apart.
+  void enqueue(int slot, cudaStream_t stream, cudaEvent_t mid = nullptr);
 
-  // Copy a host frame (row-major, height x width) into frame slot f.
-  void upload(int f, const void *host, cudaStream_t stream);
-  // Copy a device frame (row-major, pitch in bytes) into frame slot f.
-  void upload_device(int f, const void *device, size_t pitch_bytes, cudaStream_t stream);
+  // Copy a host frame (row-major, height x width) into frame f of a slot.
+  void upload(int slot, int f, const void *host, cudaStream_t stream);
+  // Copy a device frame (row-major, pitch in bytes) into frame f of a slot.
+  void upload_device(int slot, int f, const void *device, size_t pitch_bytes,
+                     cudaStream_t stream);
 
   int elem_bytes() const { return elem_bytes_; }
   int nframes() const { return static_cast<int>(shapes_.size()); }
+  int nslots() const { return static_cast<int>(slots_.size()); }
   const Shape &shape(int f) const { return shapes_[f]; }
   uint64_t pitch() const { return pitch_; }
-  void *arena() const { return arena_; }
-  // Pointer to frame f's pixel (0, 0) inside the arena.
-  void *frame_origin(int f) const;
-  SignalPixel *out() const { return out_; }
+  // Pointer to frame f's pixel (0, 0) inside slot s's arena.
+  void *frame_origin(int slot, int f) const;
+  SignalPixel *out(int slot) const { return slots_[slot].out; }
   uint64_t out_base(int f) const { return host_frames_[f].out_base; }
   uint32_t capacity(int f) const { return host_frames_[f].capacity; }
-  uint32_t *frame_count() const { return frame_count_; }
-  int *status() const { return status_; }
+  uint32_t *frame_count(int slot) const { return slots_[slot].frame_count; }
+  int *status(int slot) const { return slots_[slot].status; }
   uint32_t ntasks() const { return ntasks_; }
   uint64_t ntiles() const { return ntiles_; }
   uint64_t total_capacity() const { return total_capacity_; }
   const FrameDesc *device_frames() const { return frames_; }
-  int seg_rows() const { return seg_rows_; }
-  int warps_per_block() const { return wpc_; }
+  const PlanTuning &tuning() const { return tuning_; }
+  int grid_blocks() const { return grid_blocks_; }
+  uint64_t device_bytes() const { return device_bytes_; }
 
 private:
+  struct Slot {
+    void *arena = nullptr;
+    CUtensorMap map;
+    SignalPixel *out = nullptr;
+    uint32_t *frame_prefix = nullptr;
+    uint32_t *frame_count = nullptr; // followed by the status word
+    int *status = nullptr;
+  };
+
   void release();
 
   int elem_bytes_;
   std::vector<Shape> shapes_;
   std::vector<FrameDesc> host_frames_;
-  int seg_rows_, wpc_, blocks_per_sm_;
+  PlanTuning tuning_;
   uint64_t pitch_ = 0, arena_rows_ = 0;
   uint32_t ntasks_ = 0;
   uint64_t ntiles_ = 0, total_capacity_ = 0;
   uint32_t pool_cap_ = 0;
-  int max_blocks_ = 0;
+  int max_blocks_ = 0, grid_blocks_ = 0;
+  uint64_t device_bytes_ = 0;
 
-  CUtensorMap map_;
-  void *arena_ = nullptr;
+  std::vector<Slot> slots_;
   FrameDesc *frames_ = nullptr;
   uint32_t *tile_count_ = nullptr;
   uint32_t *tile_start_ = nullptr;
   SignalPixel *pool_ = nullptr;
-  uint32_t *pool_next_ = nullptr; // followed by the status word
-  int *status_ = nullptr;
-  SignalPixel *out_ = nullptr;
+  uint32_t *pool_next_ = nullptr;
   uint32_t *block_sums_ = nullptr;
-  uint32_t *frame_prefix_ = nullptr;
-  uint32_t *frame_count_ = nullptr;
 };
 
 } // namespace sf

@@ -27,17 +27,30 @@
 // frame and a masked pixel are treated identically by every step of the
 // reference's arithmetic (excluded from every sum, 1 in the erode input).
 //
+// Cost. The running sums are updated as if every pixel entering and leaving
+// were valid -- then the packed counts cancel and an update is one add of
+// (entering - leaving) -- and corrected afterwards for the few pixels that
+// are not (masked, or kept by the erode), only in rows where the warp holds
+// one. The dispersion test runs two pixels at a time in the sm_100 packed
+// float2 pipe, with the count converted by the exact 2^23 trick and the
+// square root taken from a table built on the device with the same
+// operation the reference uses.
+//
 // Arithmetic. Sums are exact integers; the sum of squares wraps in 32 bits
 // for 16-bit pixels (64 for 32-bit) exactly as the reference's accumulator
 // does. The two tests run in float for 16-bit pixels and double for 32-bit,
-// one IEEE rounding per operation in the reference's order, through the _rn
-// intrinsics so that nothing is contracted into an FMA.
+// one IEEE rounding per operation in the reference's order, through _rn
+// intrinsics so that nothing is contracted into an FMA (the two fma forms
+// below multiply by -1, which is exact, so each is one rounding of a
+// difference: the same as the reference's subtraction).
 //
 // Output order. Records for the tile (row, strip) land contiguously in the
 // staging pool; the tile's count and start go to two small arrays. The
 // placement kernels (place.cu) then scan the counts in row-major tile order,
 // which is ascending pixel index, and copy each tile's records to the final
 // list -- so the list comes out sorted by index with no sort.
+
+#include <math_constants.h>
 
 #include "sf_device.cuh"
 #include "sf_host.hh"
@@ -48,36 +61,79 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr uint32_t kNoChunk = 0xffffffffu;
 
+template <typename T> struct Real;
+template <> struct Real<uint16_t> { using type = float; };
+template <> struct Real<uint32_t> { using type = double; };
+
+// sqrt(2 (m - 1)) for m in [2, 63], +inf below 2: with +inf the test's right
+// side is +inf or NaN, so `lhs > rhs` is false exactly where the reference's
+// `m_sum >= 2` guard (src/dext.cc:97) is.
+__device__ __forceinline__ float sqrt_term(int m, float) {
+  return m >= 2 ? __fsqrt_rn(__fmul_rn(2.0f, __fsub_rn(__int2float_rn(m), 1.0f)))
+                : CUDART_INF_F;
+}
+__device__ __forceinline__ double sqrt_term(int m, double) {
+  return m >= 2 ? __dsqrt_rn(__dmul_rn(2.0, __dsub_rn(__int2double_rn(m), 1.0))) : CUDART_INF;
+}
+
+// An integer below 2^23 as a float, exactly: its bits OR'd under the
+// exponent of 2^23, minus 2^23.
+__device__ __forceinline__ float magic_bits(uint32_t v) {
+  return __uint_as_float(v | 0x4b000000u);
+}
+
 // --------------------------------------------------------------------------
 // The two tests, in the reference's arithmetic.
 // --------------------------------------------------------------------------
 
-// src/dext.cc:97-110 with R = float.
-__device__ __forceinline__ bool dispersion(uint32_t m, uint32_t s, uint32_t q) {
-  if (m < 2)
-    return false;
-  const float mf = __uint2float_rn(m);
-  const float sf = __uint2float_rn(s);
-  const float qf = __uint2float_rn(q);
-  const float m1 = __fsub_rn(mf, 1.0f);
-  const float lhs =
-      __fsub_rn(__fsub_rn(__fmul_rn(mf, qf), __fmul_rn(sf, sf)), __fmul_rn(sf, m1));
-  const float rhs = __fmul_rn(__fmul_rn(sf, 6.0f), __fsqrt_rn(__fmul_rn(2.0f, m1)));
-  return lhs > rhs;
+// src/dext.cc:97-110 with R = float, for the 8 columns of a lane: window
+// count+sum packed in hs (count << 22 | sum), sum of squares in hq.
+__device__ __forceinline__ uint32_t dispersion_bits(const uint32_t (&hs)[8],
+                                                    const uint32_t (&hq)[8],
+                                                    const float *sq) {
+  const float2 magic = make_float2(-8388608.0f, -8388608.0f);
+  const float2 neg1 = make_float2(-1.0f, -1.0f);
+  const float2 six = make_float2(6.0f, 6.0f);
+  uint32_t bits = 0;
+#pragma unroll
+  for (int k = 0; k < 8; k += 2) {
+    const uint32_t m0 = hs[k] >> 22, m1 = hs[k + 1] >> 22;
+    const float2 S = __fadd2_rn(make_float2(magic_bits(hs[k] & 0x3fffffu),
+                                            magic_bits(hs[k + 1] & 0x3fffffu)),
+                                magic);
+    const float2 M = __fadd2_rn(make_float2(magic_bits(m0), magic_bits(m1)), magic);
+    const float2 Q = make_float2(__uint2float_rn(hq[k]), __uint2float_rn(hq[k + 1]));
+    const float2 R = make_float2(sq[m0], sq[m1]);
+    const float2 Mm1 = __fadd2_rn(M, neg1);                   // m - 1 (exact)
+    const float2 t1 = __fmul2_rn(M, Q);                       // m * s2
+    const float2 t2 = __fmul2_rn(S, S);                       // s * s
+    const float2 t3 = __ffma2_rn(t2, neg1, t1);               // t1 - t2
+    const float2 t5 = __fmul2_rn(S, Mm1);                     // s * (m - 1)
+    const float2 lhs = __ffma2_rn(t5, neg1, t3);              // t3 - t5
+    const float2 rhs = __fmul2_rn(__fmul2_rn(S, six), R);     // s * 6 * sqrt(2(m-1))
+    bits |= (lhs.x > rhs.x ? 1u : 0u) << k;
+    bits |= (lhs.y > rhs.y ? 1u : 0u) << (k + 1);
+  }
+  return bits;
 }
 
-// The same with R = double, for 32-bit pixels.
-__device__ __forceinline__ bool dispersion(uint64_t m, uint64_t s, uint64_t q) {
-  if (m < 2)
-    return false;
-  const double md = __ull2double_rn(m);
-  const double sd = __ull2double_rn(s);
-  const double qd = __ull2double_rn(q);
-  const double m1 = __dsub_rn(md, 1.0);
-  const double lhs =
-      __dsub_rn(__dsub_rn(__dmul_rn(md, qd), __dmul_rn(sd, sd)), __dmul_rn(sd, m1));
-  const double rhs = __dmul_rn(__dmul_rn(sd, 6.0), __dsqrt_rn(__dmul_rn(2.0, m1)));
-  return lhs > rhs;
+// The same with R = double, for 32-bit pixels (count << 40 | sum).
+__device__ __forceinline__ uint32_t dispersion_bits(const uint64_t (&hs)[8],
+                                                    const uint64_t (&hq)[8],
+                                                    const double *sq) {
+  uint32_t bits = 0;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    const uint32_t m = static_cast<uint32_t>(hs[k] >> 40);
+    const double md = __uint2double_rn(m);
+    const double sd = __ull2double_rn(hs[k] & ((1ull << 40) - 1));
+    const double qd = __ull2double_rn(hq[k]);
+    const double lhs = __dsub_rn(__dsub_rn(__dmul_rn(md, qd), __dmul_rn(sd, sd)),
+                                 __dmul_rn(sd, __dsub_rn(md, 1.0)));
+    const double rhs = __dmul_rn(__dmul_rn(sd, 6.0), sq[m]);
+    bits |= (lhs > rhs ? 1u : 0u) << k;
+  }
+  return bits;
 }
 
 // src/dext.cc:200-213: mean over the masked window, then p >= mean + 3 sqrt(mean).
@@ -199,10 +255,14 @@ __global__ void __launch_bounds__(WPC * 32, 12 / WPC)
     threshold_kernel(const __grid_constant__ CUtensorMap arena, ThresholdArgs args) {
   using Tr = Traits<T>;
   using A = typename Tr::Acc;
+  using R = typename Real<T>::type;
   constexpr uint32_t kRowBytes = kStripCols * sizeof(T);
   constexpr uint32_t kBoxBytes = kRowBytes * kBoxRows;
+  constexpr A C7 = A(1) << Tr::kShift7;   // one valid pixel's count in a 7 x 7 sum
+  constexpr A C11 = A(1) << Tr::kShift11; // ... in an 11 x 11 sum
 
   extern __shared__ __align__(1024) unsigned char smem_raw[];
+  __shared__ R sqrt_tab[64];
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   T *ring = reinterpret_cast<T *>(smem_raw + warp * (kRowBytes * kRingRows));
@@ -210,12 +270,14 @@ __global__ void __launch_bounds__(WPC * 32, 12 / WPC)
       reinterpret_cast<uint64_t *>(smem_raw + WPC * (kRowBytes * kRingRows)) +
       warp * kRingStages;
 
+  for (int m = threadIdx.x; m < 64; m += blockDim.x)
+    sqrt_tab[m] = sqrt_term(m, R(0));
   if (lane == 0) {
     for (int s = 0; s < kRingStages; s++)
       mbar_init(&bars[s], 1);
     mbar_fence_init();
   }
-  __syncwarp();
+  __syncthreads();
 
   uint32_t phase = 0; // bit s = parity of the next wait on stage s
   uint32_t chunk = kNoChunk, fill = 0;
@@ -269,6 +331,8 @@ __global__ void __launch_bounds__(WPC * 32, 12 / WPC)
     uint64_t gv_lo = 0;   // valid-and-not-eroded bits, rows b .. b-7 (b = r-5)
     uint32_t gv_hi = 0;   //   rows b-8 .. b-11
     uint64_t hist_cs = 0; // candidate-region bits, rows b .. b-5
+    uint32_t dirty = 0;   // warp-uniform: bit i = row r-i holds a masked pixel
+    uint32_t gdirty = 0;  // warp-uniform: bit i = row b-i holds a non-g pixel
 
     for (int b = 0; b < nboxes && !failed; b++) {
       const int st = b % kRingStages;
@@ -293,33 +357,52 @@ __global__ void __launch_bounds__(WPC * 32, 12 / WPC)
       const int rend = min(kBoxRows, nrows - b * kBoxRows);
       for (int i = 0; i < rend; i++) {
         const int rr = b * kBoxRows + i;
-        const T *row_r = ring + (rr & (kRingRows - 1)) * kStripCols;
+        auto ring_row = [&](int back) {
+          return ring + ((rr - back) & (kRingRows - 1)) * kStripCols;
+        };
 
-        // ---- row r enters: masked bits, 7-row sums -----------------------
+        // ---- row r enters: masked bits ---------------------------------
         uint32_t p[8];
-        load_row<T>(row_r, lane, p);
+        load_row<T>(ring_row(0), lane, p);
         uint32_t mk = 0;
 #pragma unroll
         for (int k = 0; k < 8; k++)
           mk |= (p[k] >= Tr::kMasked ? 1u : 0u) << k;
+        dirty = (dirty << 1) | (__any_sync(kFull, mk != 0) ? 1u : 0u);
         hist_mk = (hist_mk << 8) | mk;
-#pragma unroll
-        for (int k = 0; k < 8; k++) {
-          const bool valid = !((mk >> k) & 1u);
-          const A pv = valid ? static_cast<A>(p[k]) : A(0);
-          vs[k] += valid ? pv + (A(1) << Tr::kShift7) : A(0);
-          vq[k] += pv * pv;
-        }
+
+        // ---- 7-row sums: + row r, - row r-7 --------------------------------
         if (rr >= 7) {
-          uint32_t q7[8];
-          load_row<T>(ring + ((rr - 7) & (kRingRows - 1)) * kStripCols, lane, q7);
-          const uint32_t mk7 = static_cast<uint32_t>(hist_mk >> 56) & 0xffu;
+          uint32_t q[8];
+          load_row<T>(ring_row(7), lane, q);
 #pragma unroll
           for (int k = 0; k < 8; k++) {
-            const bool valid = !((mk7 >> k) & 1u);
-            const A pv = valid ? static_cast<A>(q7[k]) : A(0);
-            vs[k] -= valid ? pv + (A(1) << Tr::kShift7) : A(0);
-            vq[k] -= pv * pv;
+            const A d = static_cast<A>(p[k]) - static_cast<A>(q[k]);
+            vs[k] += d;
+            vq[k] += d * (static_cast<A>(p[k]) + static_cast<A>(q[k]));
+          }
+          if (dirty & 0x81u) {
+            const uint32_t mk7 = static_cast<uint32_t>(hist_mk >> 56) & 0xffu;
+            if (mk | mk7) {
+#pragma unroll
+              for (int k = 0; k < 8; k++) {
+                if ((mk >> k) & 1u) {
+                  vs[k] -= static_cast<A>(p[k]) + C7;
+                  vq[k] -= static_cast<A>(p[k]) * static_cast<A>(p[k]);
+                }
+                if ((mk7 >> k) & 1u) {
+                  vs[k] += static_cast<A>(q[k]) + C7;
+                  vq[k] += static_cast<A>(q[k]) * static_cast<A>(q[k]);
+                }
+              }
+            }
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < 8; k++) {
+            const A v = ((mk >> k) & 1u) ? A(0) : static_cast<A>(p[k]);
+            vs[k] += ((mk >> k) & 1u) ? A(0) : v + C7;
+            vq[k] += v * v;
           }
         }
 
@@ -328,13 +411,8 @@ __global__ void __launch_bounds__(WPC * 32, 12 / WPC)
           A hs[8], hq[8];
           hsum<3>(vs, hs);
           hsum<3>(vq, hq);
-          uint32_t s0 = static_cast<uint32_t>(hist_mk >> 24) & 0xffu; // masked -> 1
-#pragma unroll
-          for (int k = 0; k < 8; k++) {
-            const A m = hs[k] >> Tr::kShift7;
-            const A s = hs[k] & ((A(1) << Tr::kShift7) - 1);
-            s0 |= (dispersion(m, s, hq[k]) ? 1u : 0u) << k;
-          }
+          const uint32_t s0 = (static_cast<uint32_t>(hist_mk >> 24) & 0xffu) | // masked -> 1
+                              dispersion_bits(hs, hq, sqrt_tab);
           hist_s0 = (hist_s0 << 8) | s0;
         }
 
@@ -353,21 +431,33 @@ __global__ void __launch_bounds__(WPC * 32, 12 / WPC)
           gv_hi = (gv_hi << 8) | static_cast<uint32_t>(gv_lo >> 56);
           gv_lo = (gv_lo << 8) | gv;
           hist_cs = (hist_cs << 8) | cs;
+          gdirty = (gdirty << 1) | (__any_sync(kFull, gv != 0xffu) ? 1u : 0u);
 
           uint32_t p5[8];
-          load_row<T>(ring + ((rr - 5) & (kRingRows - 1)) * kStripCols, lane, p5);
-#pragma unroll
-          for (int k = 0; k < 8; k++)
-            vg[k] += ((gv >> k) & 1u) ? static_cast<A>(p5[k]) + (A(1) << Tr::kShift11) : A(0);
-
+          load_row<T>(ring_row(5), lane, p5);
           if (rr >= 21) {
-            const uint32_t gv16 = (gv_hi >> 24) & 0xffu;
             uint32_t p16[8];
-            load_row<T>(ring + ((rr - 16) & (kRingRows - 1)) * kStripCols, lane, p16);
+            load_row<T>(ring_row(16), lane, p16);
 #pragma unroll
             for (int k = 0; k < 8; k++)
-              vg[k] -= ((gv16 >> k) & 1u) ? static_cast<A>(p16[k]) + (A(1) << Tr::kShift11)
-                                          : A(0);
+              vg[k] += static_cast<A>(p5[k]) - static_cast<A>(p16[k]);
+            if (gdirty & ((1u << 11) | 1u)) {
+              const uint32_t ng5 = ~gv & 0xffu;
+              const uint32_t ng16 = ~(gv_hi >> 24) & 0xffu;
+              if (ng5 | ng16) {
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                  if ((ng5 >> k) & 1u)
+                    vg[k] -= static_cast<A>(p5[k]) + C11;
+                  if ((ng16 >> k) & 1u)
+                    vg[k] += static_cast<A>(p16[k]) + C11;
+                }
+              }
+            }
+          } else {
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+              vg[k] += ((gv >> k) & 1u) ? static_cast<A>(p5[k]) + C11 : A(0);
           }
         }
 
@@ -379,17 +469,15 @@ __global__ void __launch_bounds__(WPC * 32, 12 / WPC)
             A hg[8];
             hsum<5>(vg, hg);
             uint32_t pc[8];
-            load_row<T>(ring + ((rr - kHalo) & (kRingRows - 1)) * kStripCols, lane, pc);
+            load_row<T>(ring_row(kHalo), lane, pc);
             uint32_t sig = 0;
             float bg[8];
-            uint32_t pop[8];
 #pragma unroll
             for (int k = 0; k < 8; k++) {
               bg[k] = 0.0f;
-              pop[k] = static_cast<uint32_t>(hg[k] >> Tr::kShift11);
               if (((cs >> k) & 1u) && pc[k] > 0) {
                 const A m = hg[k] >> Tr::kShift11;
-                const A s = hg[k] & ((A(1) << Tr::kShift11) - 1);
+                const A s = hg[k] & (C11 - 1);
                 if (poisson(pc[k], m, s, &bg[k]))
                   sig |= 1u << k;
               }
@@ -431,7 +519,7 @@ __global__ void __launch_bounds__(WPC * 32, 12 / WPC)
                     px.index = static_cast<uint32_t>(c) * static_cast<uint32_t>(fd.width) + col0 + k;
                     px.value = pc[k];
                     px.background = bg[k];
-                    px.population = static_cast<uint16_t>(pop[k]);
+                    px.population = static_cast<uint16_t>(hg[k] >> Tr::kShift11);
                     px.reserved = 0;
                     args.pool[at++] = px;
                   }
@@ -495,8 +583,7 @@ static cudaError_t launch_wpc(const CUtensorMap &map, const ThresholdLaunch &L,
   a.pool_cap = L.pool_cap;
   a.status = L.status;
   a.wait_limit = L.wait_limit;
-  const uint32_t warps_needed = L.ntasks;
-  uint32_t blocks = (warps_needed + WPC - 1) / WPC;
+  uint32_t blocks = (L.ntasks + WPC - 1) / WPC;
   if (L.max_blocks > 0 && blocks > static_cast<uint32_t>(L.max_blocks))
     blocks = static_cast<uint32_t>(L.max_blocks);
   if (blocks == 0)
@@ -543,8 +630,8 @@ template cudaError_t launch_threshold<uint16_t>(const CUtensorMap &, const Thres
 template cudaError_t launch_threshold<uint32_t>(const CUtensorMap &, const ThresholdLaunch &,
                                                 cudaStream_t);
 template size_t threshold_smem_bytes<uint16_t>(int);
+template size_t threshold_smem_bytes<uint32_t>(int);
 template int threshold_occupancy<uint16_t>(int);
 template int threshold_occupancy<uint32_t>(int);
-template size_t threshold_smem_bytes<uint32_t>(int);
 
 } // namespace sf

@@ -1,0 +1,120 @@
+"""The batched engine (include/spotfinder_b200.h, sf_engine_*): many frames
+of equal or uneven shapes thresholded per launch from device-resident slots,
+optionally replayed from CUDA graphs. Per frame, results are exactly
+``find()``'s (the reference's gpu::find, src/dext_gpu.hh:141-158)."""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from ._lib import SIGNAL_PIXEL, EngineConfig, lib, raise_for, require_device
+
+
+class Engine:
+    def __init__(self, shapes, dtype=np.uint16, slots=1, seg_rows=0, warps_per_block=4,
+                 blocks_per_sm=0):
+        require_device()
+        self.dtype = np.dtype(dtype)
+        if self.dtype not in (np.uint16, np.uint32):
+            raise ValueError("pixels are uint16 or uint32")
+        self.shapes = [tuple(int(v) for v in s) for s in shapes]
+        n = len(self.shapes)
+        heights = (ctypes.c_int32 * n)(*[h for h, _ in self.shapes])
+        widths = (ctypes.c_int32 * n)(*[w for _, w in self.shapes])
+        cfg = EngineConfig(seg_rows, warps_per_block, blocks_per_sm, slots)
+        handle = ctypes.c_void_p()
+        status = lib.sf_engine_create(self.dtype.itemsize, n, heights, widths,
+                                      ctypes.byref(cfg), ctypes.byref(handle))
+        raise_for(status, "sf_engine_create")
+        self._h = handle
+        self.slots = slots
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.sf_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def nframes(self):
+        return len(self.shapes)
+
+    def info(self) -> dict:
+        out = (ctypes.c_int64 * 8)()
+        raise_for(lib.sf_engine_info(self._h, out), "sf_engine_info")
+        keys = ("seg_rows", "warps_per_block", "grid_blocks", "tasks", "slots",
+                "device_bytes", "pitch", "capacity")
+        return dict(zip(keys, list(out)))
+
+    def upload(self, slot: int, frame: int, image: np.ndarray) -> None:
+        """Asynchronous host-to-device copy; keep `image` alive (and unchanged)
+        until the next synchronize()."""
+        if image.dtype != self.dtype or image.shape != self.shapes[frame]:
+            raise ValueError("frame shape or type does not match the engine")
+        if not image.flags.c_contiguous:
+            raise ValueError("frames must be C-contiguous")
+        raise_for(lib.sf_engine_upload(self._h, slot, frame, image.ctypes.data), "upload")
+
+    def upload_device(self, slot: int, frame: int, ptr: int, pitch_bytes: int) -> None:
+        raise_for(lib.sf_engine_upload_device(self._h, slot, frame, ptr, pitch_bytes),
+                  "upload_device")
+
+    def run(self, slot: int = 0) -> None:
+        raise_for(lib.sf_engine_run(self._h, slot), "run")
+
+    def use_graph(self, on: bool = True) -> None:
+        raise_for(lib.sf_engine_use_graph(self._h, int(on)), "use_graph")
+
+    def synchronize(self) -> None:
+        raise_for(lib.sf_engine_synchronize(self._h), "synchronize")
+
+    def counts(self, slot: int = 0) -> np.ndarray:
+        out = np.zeros(self.nframes, np.uint32)
+        raise_for(lib.sf_engine_counts(self._h, slot, out.ctypes.data), "counts")
+        return out
+
+    def signal_status(self, slot: int, frame: int):
+        h, w = self.shapes[frame]
+        cap = max(h * w * self.dtype.itemsize // 16, 1)
+        out = np.empty(cap, SIGNAL_PIXEL)
+        found = ctypes.c_size_t(0)
+        status = lib.sf_engine_signal(self._h, slot, frame, out.ctypes.data, cap,
+                                      ctypes.byref(found))
+        if status == -3:
+            raise_for(status, "signal")
+        if status != 0:
+            return status, np.zeros(0, SIGNAL_PIXEL)
+        return 0, out[: found.value].copy()
+
+    def signal(self, slot: int, frame: int) -> np.ndarray:
+        status, sig = self.signal_status(slot, frame)
+        raise_for(status, "signal")
+        return sig
+
+    # -- CUDA events on the engine's compute stream ------------------------
+    def record(self, mark: int) -> None:
+        raise_for(lib.sf_engine_record(self._h, mark), "record")
+
+    def elapsed_ms(self, start: int, end: int) -> float:
+        ms = ctypes.c_float(0)
+        raise_for(lib.sf_engine_elapsed(self._h, start, end, ctypes.byref(ms)), "elapsed")
+        return float(ms.value)
+
+    def profile(self, on: bool = True) -> None:
+        raise_for(lib.sf_engine_profile(self._h, int(on)), "profile")
+
+    def stage_totals(self) -> dict:
+        out = (ctypes.c_double * 4)()
+        raise_for(lib.sf_engine_stage_totals(self._h, out), "stage_totals")
+        return {"runs": int(out[0]), "threshold_ms": out[1], "place_ms": out[2],
+                "group_ms": out[3]}

@@ -92,6 +92,10 @@ SF_API void *sf_host_alloc(size_t bytes);
 SF_API void sf_host_free(void *pointer);
 /* The message for the last -3 or -4 on this thread. */
 SF_API const char *sf_last_error(void);
+/* Make `device` current for the calling thread (one process per GPU, as
+ * torchrun launches them). No reference counterpart: the reference uses the
+ * default device only. */
+SF_API int sf_set_device(int device);
 
 /* ---- the threshold: src/dext_gpu.hh:141-166 (gpu::find<T>) ------------- *
  *
@@ -117,6 +121,59 @@ SF_API int sf_find_u32(const uint32_t *image, size_t height, size_t width, sf_si
 SF_API void sf_profile_stages(int on);
 SF_API int sf_profile_stages_enabled(void);
 SF_API void sf_last_stage_times(double out6[6]);
+
+/* ---- the batched engine ------------------------------------------------- *
+ * No single reference counterpart: it replaces the reference's pattern of
+ * -j host threads each calling gpu::find on one frame (src/find_spots.cc:
+ * 472-537, src/dext_cuda.cu:585-728) with many frames -- equal or uneven
+ * shapes -- thresholded per launch from `slots` device-resident arenas.
+ * Results per frame are exactly sf_find_*'s. Uploads run on the engine's copy
+ * stream and runs on its compute stream, ordered per slot by events, so
+ * filling one slot overlaps computing another. */
+typedef struct sf_engine sf_engine;
+
+typedef struct sf_engine_config {
+  int32_t seg_rows;        /* output rows per warp task; 0 = the cost model's choice */
+  int32_t warps_per_block; /* 1, 2 or 4; 0 = 4 */
+  int32_t blocks_per_sm;   /* 0 = as many as fit */
+  int32_t slots;           /* device arenas; 0 = 1 */
+} sf_engine_config;
+
+SF_API int sf_engine_create(int elem_bytes, int nframes, const int32_t *heights,
+                            const int32_t *widths, const sf_engine_config *config,
+                            sf_engine **out);
+SF_API void sf_engine_destroy(sf_engine *engine);
+/* seg_rows, warps_per_block, grid blocks, tasks, slots, device bytes, pitch
+ * (elements), total list capacity (records). */
+SF_API int sf_engine_info(sf_engine *engine, int64_t out8[8]);
+/* Asynchronous copy of a row-major host frame (pinned for full speed) into
+ * frame `frame` of slot `slot`. */
+SF_API int sf_engine_upload(sf_engine *engine, int slot, int frame, const void *host_image);
+/* The same from device memory with a row pitch in bytes. */
+SF_API int sf_engine_upload_device(sf_engine *engine, int slot, int frame,
+                                   const void *device_image, size_t pitch_bytes);
+/* Enqueue the threshold of every frame of a slot, after its uploads. */
+SF_API int sf_engine_run(sf_engine *engine, int slot);
+/* Replay each slot's run from a CUDA graph captured on first use. */
+SF_API int sf_engine_use_graph(sf_engine *engine, int on);
+/* Wait for all enqueued work; -3 if a kernel reported a failure. */
+SF_API int sf_engine_synchronize(sf_engine *engine);
+/* Per-frame signal counts of the slot's last run (waits for it). */
+SF_API int sf_engine_counts(sf_engine *engine, int slot, uint32_t *counts);
+/* One frame's list of the slot's last run, as sf_find_* returns it,
+ * including -2 beyond the list capacity. */
+SF_API int sf_engine_signal(sf_engine *engine, int slot, int frame, sf_signal_pixel *out,
+                            size_t capacity, size_t *found);
+/* CUDA events on the compute stream: record mark 0..15; elapsed ms between
+ * two marks (waits for the later one). */
+SF_API int sf_engine_record(sf_engine *engine, int mark);
+SF_API int sf_engine_elapsed(sf_engine *engine, int from, int to, float *ms);
+/* Per-run events around the threshold kernel and the placement (outside
+ * graph replay they time each apart; inside it the two together). Turning
+ * it on resets the totals; sf_engine_stage_totals gives runs, threshold ms,
+ * placement ms, and 0, summed over the runs since. */
+SF_API int sf_engine_profile(sf_engine *engine, int on);
+SF_API int sf_engine_stage_totals(sf_engine *engine, double out4[4]);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,91 @@
+"""The batched engine through the C ABI: every frame of a batch -- equal or
+uneven shapes, either pixel type, any slot, graph replay or not -- gives
+exactly the per-frame threshold (and so the oracle's output)."""
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def frames_for(shapes, seed, dtype=np.uint16):
+    rng = np.random.default_rng(seed)
+    out = []
+    for h, w in shapes:
+        img = rng.poisson(2.0, (h, w)).astype(dtype)
+        n = max(1, h * w // 300)
+        ys, xs = rng.integers(0, h, n), rng.integers(0, w, n)
+        for y, x in zip(ys, xs):
+            img[max(0, y - 2):y + 3, max(0, x - 2):x + 3] += dtype(rng.integers(20, 5000))
+        img[rng.random((h, w)) < 0.003] = np.iinfo(dtype).max
+        out.append(img)
+    return out
+
+
+@pytest.mark.parametrize("graph", [False, True])
+def test_uneven_batch_two_slots(gpu_lib, graph):
+    from dials_metal_spotfinder_b200.engine import Engine
+    shapes = [(300, 500), (64, 90), (531, 233), (1062, 1028), (7, 3), (250, 700)]
+    batches = [frames_for(shapes, 1), frames_for(shapes, 2)]
+    with Engine(shapes, np.uint16, slots=2) as eng:
+        eng.use_graph(graph)
+        for s in range(2):
+            for f, img in enumerate(batches[s]):
+                eng.upload(s, f, img)
+        for rep in range(2):
+            for s in range(2):
+                eng.run(s)
+            eng.synchronize()
+            for s in range(2):
+                counts = eng.counts(s)
+                for f, img in enumerate(batches[s]):
+                    st, want, n = O.dext(img, capacity=img.size * 2 // 16)
+                    status, got = eng.signal_status(s, f)
+                    assert counts[f] == n
+                    assert status == st
+                    if st == 0:
+                        assert got.tobytes() == want.tobytes(), (s, f)
+
+
+def test_u32_batch(gpu_lib):
+    from dials_metal_spotfinder_b200.engine import Engine
+    shapes = [(120, 260), (200, 150)]
+    frames = frames_for(shapes, 3, np.uint32)
+    frames[0][10:14, 10:14] += np.uint32(1_500_000)
+    with Engine(shapes, np.uint32) as eng:
+        for f, img in enumerate(frames):
+            eng.upload(0, f, img)
+        eng.run(0)
+        eng.synchronize()
+        for f, img in enumerate(frames):
+            assert eng.signal(0, f).tobytes() == O.dext(img)[1].tobytes()
+
+
+@pytest.mark.parametrize("seg,wpc", [(16, 1), (37, 2), (500, 4), (0, 4)])
+def test_tunings_agree(gpu_lib, seg, wpc):
+    from dials_metal_spotfinder_b200.engine import Engine
+    shapes = [(400, 700), (333, 941)]
+    frames = frames_for(shapes, 4)
+    with Engine(shapes, np.uint16, seg_rows=seg, warps_per_block=wpc) as eng:
+        for f, img in enumerate(frames):
+            eng.upload(0, f, img)
+        eng.run(0)
+        eng.synchronize()
+        for f, img in enumerate(frames):
+            assert eng.signal(0, f).tobytes() == O.dext(img)[1].tobytes()
+
+
+def test_16m_batch_matches_oracle(gpu_lib):
+    from dials_metal_spotfinder_b200 import synth
+    from dials_metal_spotfinder_b200.engine import Engine
+    series = synth.eiger_16m(frames=4)
+    frames = [series.frame(f) for f in (0, 1)]
+    with Engine([f.shape for f in frames], np.uint16) as eng:
+        for f, img in enumerate(frames):
+            eng.upload(0, f, img)
+        eng.run(0)
+        eng.synchronize()
+        for f, img in enumerate(frames):
+            assert eng.signal(0, f).tobytes() == O.dext(img)[1].tobytes()
