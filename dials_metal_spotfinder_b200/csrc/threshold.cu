@@ -5,8 +5,8 @@
 // Decomposition. A task is one strip of 256 buffer columns (232 output
 // columns plus halo) by one segment of output rows of one frame. A warp owns
 // a task at a time and walks down it row by row; warps never talk to each
-// other. Each warp has a ring of 32 rows of its strip in shared memory, fed
-// 8 rows at a time by TMA (one elected lane issues, an mbarrier per stage).
+// other. Each warp has a ring of 24 rows of its strip in shared memory, fed
+// 4 rows at a time by TMA (one elected lane issues, an mbarrier per stage).
 //
 // Per input row r entering at the bottom of the ring, each lane (8 columns)
 // updates, all in registers:
@@ -31,18 +31,20 @@
 // were valid -- then the packed counts cancel and an update is one add of
 // (entering - leaving) -- and corrected afterwards for the few pixels that
 // are not (masked, or kept by the erode), only in rows where the warp holds
-// one. The dispersion test runs two pixels at a time in the sm_100 packed
-// float2 pipe, with the count converted by the exact 2^23 trick and the
-// square root taken from a table built on the device with the same
-// operation the reference uses.
+// one. When no pixel of the strip in the 7 rows of a dispersion window is
+// masked, every window holds 49 pixels and the test runs with m = 49 as
+// constants; otherwise m, and the square root from a table built on the
+// device with the reference's own operation, vary per pixel. Either way the
+// test runs two pixels at a time in the sm_100 packed float2 pipe.
 //
 // Arithmetic. Sums are exact integers; the sum of squares wraps in 32 bits
 // for 16-bit pixels (64 for 32-bit) exactly as the reference's accumulator
 // does. The two tests run in float for 16-bit pixels and double for 32-bit,
 // one IEEE rounding per operation in the reference's order, through _rn
-// intrinsics so that nothing is contracted into an FMA (the two fma forms
-// below multiply by -1, which is exact, so each is one rounding of a
-// difference: the same as the reference's subtraction).
+// intrinsics so that nothing is contracted into an FMA (the fma forms below
+// multiply by -1, which is exact, so each is one rounding of a difference:
+// the same as the reference's subtraction). `lhs > rhs` is read off the sign
+// of the correctly rounded rhs - lhs, which rounding cannot flip.
 //
 // Output order. Records for the tile (row, strip) land contiguously in the
 // staging pool; the tile's count and start go to two small arrays. The
@@ -51,6 +53,8 @@
 // list -- so the list comes out sorted by index with no sort.
 
 #include <math_constants.h>
+
+#include <type_traits>
 
 #include "sf_device.cuh"
 #include "sf_host.hh"
@@ -76,10 +80,15 @@ __device__ __forceinline__ double sqrt_term(int m, double) {
   return m >= 2 ? __dsqrt_rn(__dmul_rn(2.0, __dsub_rn(__int2double_rn(m), 1.0))) : CUDART_INF;
 }
 
-// An integer below 2^23 as a float, exactly: its bits OR'd under the
-// exponent of 2^23, minus 2^23.
+// An integer below 2^23 with its bits OR'd under the exponent of 2^23: as a
+// float that is 2^23 + v exactly.
 __device__ __forceinline__ float magic_bits(uint32_t v) {
   return __uint_as_float(v | 0x4b000000u);
+}
+
+// Shifts `bits` left by one and brings in the sign bit of `x`.
+__device__ __forceinline__ uint32_t push_sign(uint32_t bits, float x) {
+  return __funnelshift_l(__float_as_uint(x), bits, 1);
 }
 
 // --------------------------------------------------------------------------
@@ -87,7 +96,8 @@ __device__ __forceinline__ float magic_bits(uint32_t v) {
 // --------------------------------------------------------------------------
 
 // src/dext.cc:97-110 with R = float, for the 8 columns of a lane: window
-// count+sum packed in hs (count << 22 | sum), sum of squares in hq.
+// count+sum packed in hs (count << 22 | sum), sum of squares in hq. `sq` is
+// the per-count table (sqrt_term). Bit k set where the window is dispersed.
 __device__ __forceinline__ uint32_t dispersion_bits(const uint32_t (&hs)[8],
                                                     const uint32_t (&hq)[8],
                                                     const float *sq) {
@@ -96,7 +106,7 @@ __device__ __forceinline__ uint32_t dispersion_bits(const uint32_t (&hs)[8],
   const float2 six = make_float2(6.0f, 6.0f);
   uint32_t bits = 0;
 #pragma unroll
-  for (int k = 0; k < 8; k += 2) {
+  for (int k = 6; k >= 0; k -= 2) {
     const uint32_t m0 = hs[k] >> 22, m1 = hs[k + 1] >> 22;
     const float2 S = __fadd2_rn(make_float2(magic_bits(hs[k] & 0x3fffffu),
                                             magic_bits(hs[k + 1] & 0x3fffffu)),
@@ -111,8 +121,39 @@ __device__ __forceinline__ uint32_t dispersion_bits(const uint32_t (&hs)[8],
     const float2 t5 = __fmul2_rn(S, Mm1);                     // s * (m - 1)
     const float2 lhs = __ffma2_rn(t5, neg1, t3);              // t3 - t5
     const float2 rhs = __fmul2_rn(__fmul2_rn(S, six), R);     // s * 6 * sqrt(2(m-1))
-    bits |= (lhs.x > rhs.x ? 1u : 0u) << k;
-    bits |= (lhs.y > rhs.y ? 1u : 0u) << (k + 1);
+    const float2 d = __ffma2_rn(lhs, neg1, rhs);              // rhs - lhs
+    bits = push_sign(bits, d.y);
+    bits = push_sign(bits, d.x);
+  }
+  return bits;
+}
+
+// The same when every window holds 49 pixels: m, m - 1 and the square root
+// are constants (sq49 = sqrt_term(49)).
+__device__ __forceinline__ uint32_t dispersion_bits49(const uint32_t (&hs)[8],
+                                                      const uint32_t (&hq)[8], float sq49) {
+  const float2 magic = make_float2(-8388608.0f, -8388608.0f);
+  const float2 neg1 = make_float2(-1.0f, -1.0f);
+  const float2 six = make_float2(6.0f, 6.0f);
+  const float2 c49 = make_float2(49.0f, 49.0f);
+  const float2 c48 = make_float2(48.0f, 48.0f);
+  const float2 R = make_float2(sq49, sq49);
+  uint32_t bits = 0;
+#pragma unroll
+  for (int k = 6; k >= 0; k -= 2) {
+    const float2 S = __fadd2_rn(make_float2(magic_bits(hs[k] & 0x3fffffu),
+                                            magic_bits(hs[k + 1] & 0x3fffffu)),
+                                magic);
+    const float2 Q = make_float2(__uint2float_rn(hq[k]), __uint2float_rn(hq[k + 1]));
+    const float2 t1 = __fmul2_rn(c49, Q);
+    const float2 t2 = __fmul2_rn(S, S);
+    const float2 t3 = __ffma2_rn(t2, neg1, t1);
+    const float2 t5 = __fmul2_rn(S, c48);
+    const float2 lhs = __ffma2_rn(t5, neg1, t3);
+    const float2 rhs = __fmul2_rn(__fmul2_rn(S, six), R);
+    const float2 d = __ffma2_rn(lhs, neg1, rhs);
+    bits = push_sign(bits, d.y);
+    bits = push_sign(bits, d.x);
   }
   return bits;
 }
@@ -157,27 +198,55 @@ __device__ __forceinline__ bool poisson(uint32_t p, uint64_t m, uint64_t s,
 // Row access
 // --------------------------------------------------------------------------
 
-// The lane's 8 pixels of one ring row.
+// The lane's 8 pixels of one ring row, and whether any is masked.
+template <typename T> struct LaneRow;
+
+template <> struct LaneRow<uint16_t> {
+  uint4 v;
+  __device__ __forceinline__ void load(const uint16_t *row, int lane) {
+    v = reinterpret_cast<const uint4 *>(row)[lane];
+  }
+  __device__ __forceinline__ void unpack(uint32_t (&p)[8]) const {
+    p[0] = v.x & 0xffffu; p[1] = v.x >> 16;
+    p[2] = v.y & 0xffffu; p[3] = v.y >> 16;
+    p[4] = v.z & 0xffffu; p[5] = v.z >> 16;
+    p[6] = v.w & 0xffffu; p[7] = v.w >> 16;
+  }
+  // Nonzero iff a pixel is 0xfffe or 0xffff: such a half is all ones once
+  // its low bit is set, so its complement is a zero half, which the borrow
+  // of a 16-bit subtract finds.
+  __device__ __forceinline__ uint32_t any_masked() const {
+    auto z = [](uint32_t w) {
+      const uint32_t b = ~(w | 0x00010001u);
+      return (b - 0x00010001u) & ~b & 0x80008000u;
+    };
+    return z(v.x) | z(v.y) | z(v.z) | z(v.w);
+  }
+};
+
+template <> struct LaneRow<uint32_t> {
+  uint4 a, b;
+  __device__ __forceinline__ void load(const uint32_t *row, int lane) {
+    const uint4 *v = reinterpret_cast<const uint4 *>(row + 8 * lane);
+    a = v[0];
+    b = v[1];
+  }
+  __device__ __forceinline__ void unpack(uint32_t (&p)[8]) const {
+    p[0] = a.x; p[1] = a.y; p[2] = a.z; p[3] = a.w;
+    p[4] = b.x; p[5] = b.y; p[6] = b.z; p[7] = b.w;
+  }
+  __device__ __forceinline__ uint32_t any_masked() const {
+    const uint32_t m = Traits<uint32_t>::kMasked;
+    return (a.x >= m) | (a.y >= m) | (a.z >= m) | (a.w >= m) | (b.x >= m) | (b.y >= m) |
+           (b.z >= m) | (b.w >= m);
+  }
+};
+
 template <typename T>
-__device__ __forceinline__ void load_row(const T *row, int lane, uint32_t (&p)[8]);
-
-template <>
-__device__ __forceinline__ void load_row<uint16_t>(const uint16_t *row, int lane,
-                                                   uint32_t (&p)[8]) {
-  const uint4 v = reinterpret_cast<const uint4 *>(row)[lane];
-  p[0] = v.x & 0xffffu; p[1] = v.x >> 16;
-  p[2] = v.y & 0xffffu; p[3] = v.y >> 16;
-  p[4] = v.z & 0xffffu; p[5] = v.z >> 16;
-  p[6] = v.w & 0xffffu; p[7] = v.w >> 16;
-}
-
-template <>
-__device__ __forceinline__ void load_row<uint32_t>(const uint32_t *row, int lane,
-                                                   uint32_t (&p)[8]) {
-  const uint4 *v = reinterpret_cast<const uint4 *>(row + 8 * lane);
-  const uint4 a = v[0], b = v[1];
-  p[0] = a.x; p[1] = a.y; p[2] = a.z; p[3] = a.w;
-  p[4] = b.x; p[5] = b.y; p[6] = b.z; p[7] = b.w;
+__device__ __forceinline__ void load_pixels(const T *row, int lane, uint32_t (&p)[8]) {
+  LaneRow<T> r;
+  r.load(row, lane);
+  r.unpack(p);
 }
 
 __device__ __forceinline__ uint32_t shfl_up(uint32_t v) { return __shfl_up_sync(kFull, v, 1); }
@@ -250,34 +319,50 @@ __device__ __forceinline__ int find_frame(const FrameDesc *frames, int n,
   return lo;
 }
 
+// Ring slot of the row `back` rows above the row in slot `slot`.
+__device__ __forceinline__ int back_slot(int slot, int back) {
+  const int s = slot - back;
+  return s < 0 ? s + kRingRows : s;
+}
+
+// 16 warps per SM for 16-bit pixels (12 KB rings); 32-bit rings are twice
+// the size, so 8 warps fit and the registers can be spent instead.
 template <typename T, int WPC>
-__global__ void __launch_bounds__(WPC * 32, 12 / WPC)
+__global__ void __launch_bounds__(WPC * 32, (sizeof(T) == 2 ? 16 : 8) / WPC)
     threshold_kernel(const __grid_constant__ CUtensorMap arena, ThresholdArgs args) {
   using Tr = Traits<T>;
   using A = typename Tr::Acc;
-  using R = typename Real<T>::type;
+  using Rl = typename Real<T>::type;
   constexpr uint32_t kRowBytes = kStripCols * sizeof(T);
   constexpr uint32_t kBoxBytes = kRowBytes * kBoxRows;
   constexpr A C7 = A(1) << Tr::kShift7;   // one valid pixel's count in a 7 x 7 sum
   constexpr A C11 = A(1) << Tr::kShift11; // ... in an 11 x 11 sum
+  constexpr int kWarmup = 21;             // rows before every stage is live
 
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  __shared__ R sqrt_tab[64];
+  __shared__ Rl sqrt_tab[64];
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  T *ring = reinterpret_cast<T *>(smem_raw + warp * (kRowBytes * kRingRows));
-  uint64_t *bars =
-      reinterpret_cast<uint64_t *>(smem_raw + WPC * (kRowBytes * kRingRows)) +
-      warp * kRingStages;
+  // Per warp: the ring, the 11 x 11 window sums of one row (for the
+  // candidates), the stage barriers and the candidate column list.
+  unsigned char *at = smem_raw;
+  T *ring = reinterpret_cast<T *>(at + warp * (kRowBytes * kRingRows));
+  at += WPC * (kRowBytes * kRingRows);
+  A *win11 = reinterpret_cast<A *>(at) + warp * kStripCols;
+  at += WPC * kStripCols * sizeof(A);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(at) + warp * kRingStages;
+  at += WPC * kRingStages * sizeof(uint64_t);
+  uint8_t *cand_col = at + warp * kStripCols;
 
   for (int m = threadIdx.x; m < 64; m += blockDim.x)
-    sqrt_tab[m] = sqrt_term(m, R(0));
+    sqrt_tab[m] = sqrt_term(m, Rl(0));
   if (lane == 0) {
     for (int s = 0; s < kRingStages; s++)
       mbar_init(&bars[s], 1);
     mbar_fence_init();
   }
   __syncthreads();
+  const float sq49 = static_cast<float>(sqrt_tab[49]);
 
   uint32_t phase = 0; // bit s = parity of the next wait on stage s
   uint32_t chunk = kNoChunk, fill = 0;
@@ -334,10 +419,216 @@ __global__ void __launch_bounds__(WPC * 32, 12 / WPC)
     uint32_t dirty = 0;   // warp-uniform: bit i = row r-i holds a masked pixel
     uint32_t gdirty = 0;  // warp-uniform: bit i = row b-i holds a non-g pixel
 
+    auto row_at = [&](int slot) { return ring + slot * kStripCols; };
+
+    // One input row: `rr` rows into the task, in ring slot `slot`. With
+    // `steady`, rr >= kWarmup and every stage runs unconditionally.
+    auto process_row = [&](int rr, int slot, auto steady_tag) {
+      constexpr bool steady = decltype(steady_tag)::value;
+
+      // ---- row r enters: masked bits -----------------------------------
+      LaneRow<T> raw;
+      raw.load(row_at(slot), lane);
+      uint32_t p[8];
+      raw.unpack(p);
+      uint32_t mk = 0;
+      const bool rdirty = __any_sync(kFull, raw.any_masked() != 0);
+      if (rdirty) {
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+          mk |= (p[k] >= Tr::kMasked ? 1u : 0u) << k;
+      }
+      dirty = (dirty << 1) | (rdirty ? 1u : 0u);
+      hist_mk = (hist_mk << 8) | mk;
+
+      // ---- 7-row sums: + row r, - row r-7 --------------------------------
+      if (steady || rr >= 7) {
+        uint32_t q[8];
+        load_pixels<T>(row_at(back_slot(slot, 7)), lane, q);
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          const A d = static_cast<A>(p[k]) - static_cast<A>(q[k]);
+          vs[k] += d;
+          vq[k] += d * (static_cast<A>(p[k]) + static_cast<A>(q[k]));
+        }
+        if (dirty & 0x81u) {
+          const uint32_t mk7 = static_cast<uint32_t>(hist_mk >> 56) & 0xffu;
+          if (mk | mk7) {
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+              if ((mk >> k) & 1u) {
+                vs[k] -= static_cast<A>(p[k]) + C7;
+                vq[k] -= static_cast<A>(p[k]) * static_cast<A>(p[k]);
+              }
+              if ((mk7 >> k) & 1u) {
+                vs[k] += static_cast<A>(q[k]) + C7;
+                vq[k] += static_cast<A>(q[k]) * static_cast<A>(q[k]);
+              }
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < 8; k++) {
+          const A v = ((mk >> k) & 1u) ? A(0) : static_cast<A>(p[k]);
+          vs[k] += ((mk >> k) & 1u) ? A(0) : v + C7;
+          vq[k] += v * v;
+        }
+      }
+
+      // ---- dispersion test at row a = r-3 ------------------------------
+      if (steady || rr >= 6) {
+        A hs[8], hq[8];
+        hsum<3>(vs, hs);
+        hsum<3>(vq, hq);
+        uint32_t bits;
+        if constexpr (sizeof(T) == 2) {
+          bits = (dirty & 0x7fu) ? dispersion_bits(hs, hq, sqrt_tab)
+                                 : dispersion_bits49(hs, hq, sq49);
+        } else {
+          bits = dispersion_bits(hs, hq, sqrt_tab);
+        }
+        const uint32_t s0 = (static_cast<uint32_t>(hist_mk >> 24) & 0xffu) | bits; // masked -> 1
+        hist_s0 = (hist_s0 << 8) | s0;
+      }
+
+      // ---- erode at row b = r-5, and the 11-row sums -------------------
+      if (steady || rr >= 10) {
+        const uint32_t v = static_cast<uint32_t>(hist_s0 & (hist_s0 >> 8) &
+                                                 (hist_s0 >> 16) & (hist_s0 >> 24) &
+                                                 (hist_s0 >> 32)) & 0xffu;
+        const uint32_t vl = shfl_up(v), vr = shfl_down(v);
+        const uint32_t w = (vl >> 6) | (v << 2) | (vr << 10);
+        const uint32_t hv = w & (w >> 1) & (w >> 2) & (w >> 3) & (w >> 4) & 0xffu;
+        const uint32_t mkb = static_cast<uint32_t>(hist_mk >> 40) & 0xffu;
+        const uint32_t s1 = hv | mkb;           // scr1, src/dext.cc:117-142
+        const uint32_t gv = ~s1 & 0xffu;        // valid and not kept
+        const uint32_t cs = s1 & ~mkb & 0xffu;  // kept and not masked
+        gv_hi = (gv_hi << 8) | static_cast<uint32_t>(gv_lo >> 56);
+        gv_lo = (gv_lo << 8) | gv;
+        hist_cs = (hist_cs << 8) | cs;
+        gdirty = (gdirty << 1) | (__any_sync(kFull, gv != 0xffu) ? 1u : 0u);
+
+        uint32_t p5[8];
+        load_pixels<T>(row_at(back_slot(slot, 5)), lane, p5);
+        if (steady || rr >= kWarmup) {
+          uint32_t p16[8];
+          load_pixels<T>(row_at(back_slot(slot, 16)), lane, p16);
+#pragma unroll
+          for (int k = 0; k < 8; k++)
+            vg[k] += static_cast<A>(p5[k]) - static_cast<A>(p16[k]);
+          if (gdirty & ((1u << 11) | 1u)) {
+            const uint32_t ng5 = ~gv & 0xffu;
+            const uint32_t ng16 = ~(gv_hi >> 24) & 0xffu;
+            if (ng5 | ng16) {
+#pragma unroll
+              for (int k = 0; k < 8; k++) {
+                if ((ng5 >> k) & 1u)
+                  vg[k] -= static_cast<A>(p5[k]) + C11;
+                if ((ng16 >> k) & 1u)
+                  vg[k] += static_cast<A>(p16[k]) + C11;
+              }
+            }
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < 8; k++)
+            vg[k] += ((gv >> k) & 1u) ? static_cast<A>(p5[k]) + C11 : A(0);
+        }
+      }
+
+      // ---- Poisson test and emit at row c = r-10 -----------------------
+      if (steady || rr >= 2 * kHalo) {
+        const int c = rs + rr - kHalo; // frame row of the output
+        const uint32_t cs = static_cast<uint32_t>(hist_cs >> 40) & 0xffu & outmask;
+        if (__any_sync(kFull, cs != 0)) {
+          // The candidates are compacted one per lane before the Poisson
+          // test, so each pays for one division and one square root
+          // instead of every lane paying for all eight columns.
+          A hg[8];
+          hsum<5>(vg, hg);
+#pragma unroll
+          for (int k = 0; k < 8; k++)
+            win11[8 * lane + k] = hg[k];
+          // The candidate columns in ascending order: lane by lane, and
+          // within a lane by column.
+          const uint32_t cnt = __popc(cs);
+          uint32_t incl = cnt;
+#pragma unroll
+          for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t t = __shfl_up_sync(kFull, incl, d);
+            if (lane >= d)
+              incl += t;
+          }
+          const uint32_t total = __shfl_sync(kFull, incl, 31);
+          {
+            uint32_t at = incl - cnt, left = cs;
+            while (left) {
+              cand_col[at++] = static_cast<uint8_t>(8 * lane + __ffs(left) - 1);
+              left &= left - 1;
+            }
+          }
+          __syncwarp();
+
+          // Room for every candidate in one chunk, so the tile's records
+          // are contiguous whatever the rounds below find.
+          if (chunk == kNoChunk || fill + total > kChunkRecords) {
+            uint32_t base = 0;
+            if (lane == 0)
+              base = atomicAdd(args.pool_next, kChunkRecords);
+            base = __shfl_sync(kFull, base, 0);
+            if (base > args.pool_cap - kChunkRecords || base + kChunkRecords < base) {
+              if (lane == 0)
+                atomicCAS(args.status, kStatusOk, kStatusPoolExhausted);
+              chunk = kNoChunk;
+            } else {
+              chunk = base;
+            }
+            fill = 0;
+          }
+          const uint32_t start = chunk + fill;
+          const T *prow = row_at(back_slot(slot, kHalo));
+          const uint32_t row_index = static_cast<uint32_t>(c) * static_cast<uint32_t>(fd.width) +
+                                     static_cast<uint32_t>(strip * kStripOut - kHalo);
+          uint32_t found = 0;
+          for (uint32_t base = 0; base < total; base += 32) {
+            const uint32_t i = base + lane;
+            bool sig = false;
+            SignalPixel px;
+            if (i < total) {
+              const uint32_t col = cand_col[i];
+              const uint32_t p = prow[col];
+              const A h = win11[col];
+              if (p > 0) { // a masked pixel is never a candidate
+                sig = poisson(p, h >> Tr::kShift11, h & (C11 - 1), &px.background);
+                px.index = row_index + col;
+                px.value = p;
+                px.population = static_cast<uint16_t>(h >> Tr::kShift11);
+                px.reserved = 0;
+              }
+            }
+            const uint32_t ball = __ballot_sync(kFull, sig);
+            if (sig && chunk != kNoChunk)
+              args.pool[start + found + __popc(ball & ((1u << lane) - 1u))] = px;
+            found += __popc(ball);
+          }
+          if (found > 0) {
+            fill += found;
+            if (lane == 0) {
+              const uint64_t tile = fd.tile_base + static_cast<uint64_t>(c) * fd.strips + strip;
+              args.tile_count[tile] = found; // counted even if the records were dropped
+              args.tile_start[tile] = chunk == kNoChunk ? 0u : start;
+            }
+          }
+          __syncwarp();
+        }
+      }
+    };
+
     for (int b = 0; b < nboxes && !failed; b++) {
       const int st = b % kRingStages;
       if (lane == 0 && b >= 1 && b + 1 < nboxes) {
-        // Box b+1 reuses the stage of box b-3, whose rows are all older than
+        // Box b+1 reuses the stage of box b-5, whose rows are all older than
         // r-16 for every row of box b: free.
         const int nst = (b + 1) % kRingStages;
         fence_proxy_async_smem();
@@ -354,188 +645,14 @@ __global__ void __launch_bounds__(WPC * 32, 12 / WPC)
         break;
       }
 
-      const int rend = min(kBoxRows, nrows - b * kBoxRows);
-      for (int i = 0; i < rend; i++) {
-        const int rr = b * kBoxRows + i;
-        auto ring_row = [&](int back) {
-          return ring + ((rr - back) & (kRingRows - 1)) * kStripCols;
-        };
-
-        // ---- row r enters: masked bits ---------------------------------
-        uint32_t p[8];
-        load_row<T>(ring_row(0), lane, p);
-        uint32_t mk = 0;
-#pragma unroll
-        for (int k = 0; k < 8; k++)
-          mk |= (p[k] >= Tr::kMasked ? 1u : 0u) << k;
-        dirty = (dirty << 1) | (__any_sync(kFull, mk != 0) ? 1u : 0u);
-        hist_mk = (hist_mk << 8) | mk;
-
-        // ---- 7-row sums: + row r, - row r-7 --------------------------------
-        if (rr >= 7) {
-          uint32_t q[8];
-          load_row<T>(ring_row(7), lane, q);
-#pragma unroll
-          for (int k = 0; k < 8; k++) {
-            const A d = static_cast<A>(p[k]) - static_cast<A>(q[k]);
-            vs[k] += d;
-            vq[k] += d * (static_cast<A>(p[k]) + static_cast<A>(q[k]));
-          }
-          if (dirty & 0x81u) {
-            const uint32_t mk7 = static_cast<uint32_t>(hist_mk >> 56) & 0xffu;
-            if (mk | mk7) {
-#pragma unroll
-              for (int k = 0; k < 8; k++) {
-                if ((mk >> k) & 1u) {
-                  vs[k] -= static_cast<A>(p[k]) + C7;
-                  vq[k] -= static_cast<A>(p[k]) * static_cast<A>(p[k]);
-                }
-                if ((mk7 >> k) & 1u) {
-                  vs[k] += static_cast<A>(q[k]) + C7;
-                  vq[k] += static_cast<A>(q[k]) * static_cast<A>(q[k]);
-                }
-              }
-            }
-          }
-        } else {
-#pragma unroll
-          for (int k = 0; k < 8; k++) {
-            const A v = ((mk >> k) & 1u) ? A(0) : static_cast<A>(p[k]);
-            vs[k] += ((mk >> k) & 1u) ? A(0) : v + C7;
-            vq[k] += v * v;
-          }
-        }
-
-        // ---- dispersion test at row a = r-3 ------------------------------
-        if (rr >= 6) {
-          A hs[8], hq[8];
-          hsum<3>(vs, hs);
-          hsum<3>(vq, hq);
-          const uint32_t s0 = (static_cast<uint32_t>(hist_mk >> 24) & 0xffu) | // masked -> 1
-                              dispersion_bits(hs, hq, sqrt_tab);
-          hist_s0 = (hist_s0 << 8) | s0;
-        }
-
-        // ---- erode at row b = r-5, and the 11-row sums -------------------
-        if (rr >= 10) {
-          const uint32_t v = static_cast<uint32_t>(hist_s0 & (hist_s0 >> 8) &
-                                                   (hist_s0 >> 16) & (hist_s0 >> 24) &
-                                                   (hist_s0 >> 32)) & 0xffu;
-          const uint32_t vl = shfl_up(v), vr = shfl_down(v);
-          const uint32_t w = (vl >> 6) | (v << 2) | (vr << 10);
-          const uint32_t hv = w & (w >> 1) & (w >> 2) & (w >> 3) & (w >> 4) & 0xffu;
-          const uint32_t mkb = static_cast<uint32_t>(hist_mk >> 40) & 0xffu;
-          const uint32_t s1 = hv | mkb;           // scr1, src/dext.cc:117-142
-          const uint32_t gv = ~s1 & 0xffu;        // valid and not kept
-          const uint32_t cs = s1 & ~mkb & 0xffu;  // kept and not masked
-          gv_hi = (gv_hi << 8) | static_cast<uint32_t>(gv_lo >> 56);
-          gv_lo = (gv_lo << 8) | gv;
-          hist_cs = (hist_cs << 8) | cs;
-          gdirty = (gdirty << 1) | (__any_sync(kFull, gv != 0xffu) ? 1u : 0u);
-
-          uint32_t p5[8];
-          load_row<T>(ring_row(5), lane, p5);
-          if (rr >= 21) {
-            uint32_t p16[8];
-            load_row<T>(ring_row(16), lane, p16);
-#pragma unroll
-            for (int k = 0; k < 8; k++)
-              vg[k] += static_cast<A>(p5[k]) - static_cast<A>(p16[k]);
-            if (gdirty & ((1u << 11) | 1u)) {
-              const uint32_t ng5 = ~gv & 0xffu;
-              const uint32_t ng16 = ~(gv_hi >> 24) & 0xffu;
-              if (ng5 | ng16) {
-#pragma unroll
-                for (int k = 0; k < 8; k++) {
-                  if ((ng5 >> k) & 1u)
-                    vg[k] -= static_cast<A>(p5[k]) + C11;
-                  if ((ng16 >> k) & 1u)
-                    vg[k] += static_cast<A>(p16[k]) + C11;
-                }
-              }
-            }
-          } else {
-#pragma unroll
-            for (int k = 0; k < 8; k++)
-              vg[k] += ((gv >> k) & 1u) ? static_cast<A>(p5[k]) + C11 : A(0);
-          }
-        }
-
-        // ---- Poisson test and emit at row c = r-10 -----------------------
-        if (rr >= 2 * kHalo) {
-          const int c = rs + rr - kHalo; // frame row of the output
-          const uint32_t cs = static_cast<uint32_t>(hist_cs >> 40) & 0xffu & outmask;
-          if (__any_sync(kFull, cs != 0)) {
-            A hg[8];
-            hsum<5>(vg, hg);
-            uint32_t pc[8];
-            load_row<T>(ring_row(kHalo), lane, pc);
-            uint32_t sig = 0;
-            float bg[8];
-#pragma unroll
-            for (int k = 0; k < 8; k++) {
-              bg[k] = 0.0f;
-              if (((cs >> k) & 1u) && pc[k] > 0) {
-                const A m = hg[k] >> Tr::kShift11;
-                const A s = hg[k] & (C11 - 1);
-                if (poisson(pc[k], m, s, &bg[k]))
-                  sig |= 1u << k;
-              }
-            }
-            const uint32_t cnt = __popc(sig);
-            uint32_t incl = cnt;
-#pragma unroll
-            for (int d = 1; d < 32; d <<= 1) {
-              const uint32_t t = __shfl_up_sync(kFull, incl, d);
-              if (lane >= d)
-                incl += t;
-            }
-            const uint32_t total = __shfl_sync(kFull, incl, 31);
-            if (total > 0) {
-              if (chunk == kNoChunk || fill + total > kChunkRecords) {
-                uint32_t base = 0;
-                if (lane == 0)
-                  base = atomicAdd(args.pool_next, kChunkRecords);
-                base = __shfl_sync(kFull, base, 0);
-                if (base > args.pool_cap - kChunkRecords || base + kChunkRecords < base) {
-                  if (lane == 0)
-                    atomicCAS(args.status, kStatusOk, kStatusPoolExhausted);
-                  chunk = kNoChunk;
-                } else {
-                  chunk = base;
-                }
-                fill = 0;
-              }
-              const uint64_t tile = fd.tile_base + static_cast<uint64_t>(c) * fd.strips + strip;
-              if (chunk != kNoChunk) {
-                const uint32_t start = chunk + fill;
-                fill += total;
-                uint32_t at = start + (incl - cnt);
-                const uint32_t col0 = strip * kStripOut + 8 * lane - kHalo;
-#pragma unroll
-                for (int k = 0; k < 8; k++) {
-                  if ((sig >> k) & 1u) {
-                    SignalPixel px;
-                    px.index = static_cast<uint32_t>(c) * static_cast<uint32_t>(fd.width) + col0 + k;
-                    px.value = pc[k];
-                    px.background = bg[k];
-                    px.population = static_cast<uint16_t>(hg[k] >> Tr::kShift11);
-                    px.reserved = 0;
-                    args.pool[at++] = px;
-                  }
-                }
-                if (lane == 0) {
-                  args.tile_count[tile] = total;
-                  args.tile_start[tile] = start;
-                }
-              } else if (lane == 0) {
-                args.tile_count[tile] = total; // counted, records dropped
-                args.tile_start[tile] = 0;
-              }
-            }
-          }
-        }
-      }
+      // One copy of the row body: a second (say, a warm-up-free steady
+      // state) doubles the code and the instruction cache then misses.
+      const int rr0 = b * kBoxRows;
+      const int slot0 = st * kBoxRows;
+      const int rend = min(kBoxRows, nrows - rr0);
+#pragma unroll 1
+      for (int i = 0; i < rend; i++)
+        process_row(rr0 + i, slot0 + i, std::false_type{});
       __syncwarp();
     }
     if (failed) {
@@ -555,8 +672,10 @@ __global__ void __launch_bounds__(WPC * 32, 12 / WPC)
 
 template <typename T>
 size_t threshold_smem_bytes(int wpc) {
-  return static_cast<size_t>(wpc) * (kStripCols * sizeof(T) * kRingRows) +
-         static_cast<size_t>(wpc) * kRingStages * sizeof(uint64_t);
+  using A = typename Traits<T>::Acc;
+  return static_cast<size_t>(wpc) *
+         (kStripCols * sizeof(T) * kRingRows + kStripCols * sizeof(A) +
+          kRingStages * sizeof(uint64_t) + kStripCols);
 }
 
 template <typename T, int WPC>
