@@ -53,7 +53,11 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch", type=int, default=16)
-    ap.add_argument("--pool", type=int, default=8, help="distinct synthetic frames")
+    # Distinct consecutive frames of one series, cycled. With grouping in the
+    # step the cycle must be longer than any reflection's extent in z (about
+    # ten frames here): a reflection present at both ends of a short cycle
+    # would be joined across the wrap into a streak that never closes.
+    ap.add_argument("--pool", type=int, default=32, help="distinct synthetic frames")
     ap.add_argument("--e2e-steps", type=int, default=4)
     ap.add_argument("--cpu-frames", type=int, default=8)
     ap.add_argument("--no-cpu", action="store_true")
@@ -254,6 +258,7 @@ def run_ours(args, ranks):
     pool = make_pool(args.pool)
     frame_bytes = SHAPE[0] * SHAPE[1] * 2
     eng = Engine([SHAPE] * F, np.uint16, slots=2)
+    eng.enable_grouping(first_frame=0)
     info = eng.info()
     for s in range(2):
         for f in range(F):
@@ -265,7 +270,8 @@ def run_ours(args, ranks):
         eng.run(i % 2)
     eng.synchronize()
 
-    # timed: resident frames
+    # timed: resident frames, the whole step (threshold, ordered compaction,
+    # 3D grouping and the spot pass) on the device
     eng.profile(True)
     ranks.barrier()
     with ClockSampler(ranks.local) as clocks:
@@ -281,8 +287,22 @@ def run_ours(args, ranks):
     eng.profile(False)
     counts = [eng.counts(s) for s in range(2)]
     nsig_per_step = [int(c.sum()) for c in counts]
+    group_counts, live = eng.group_counts()
     frames_total = ranks.sum(F * args.steps)
     value = frames_total / (ms_max / 1000.0)
+
+    # the same steps replayed from CUDA graphs
+    eng.use_graph(True)
+    for i in range(2):
+        eng.run(i % 2)
+    eng.synchronize()
+    eng.record(2)
+    for i in range(args.steps):
+        eng.run(i % 2)
+    eng.record(3)
+    eng.synchronize()
+    graph_ms = ranks.max(eng.elapsed_ms(2, 3))
+    eng.use_graph(False)
 
     # roofline of the threshold kernel: algorithmic bytes per launch (one read
     # of every frame plus one 16-byte record per signal pixel) over the
@@ -299,22 +319,18 @@ def run_ours(args, ranks):
         hb = [sf.HostBuffer(SHAPE, np.uint16) for _ in range(F)]
         for f in range(F):
             hb[f].array[:] = pool[f % len(pool)]
-        sig_buf = np.empty(frame_bytes // 16, sf.SIGNAL_PIXEL)
         d2h = 0
 
         def e2e_step(slot):
+            # frames in from pinned host memory; the step's finished spots and
+            # their pixels back to the host
             nonlocal d2h
             for f in range(F):
                 eng.upload(slot, f, hb[f].array)
             eng.run(slot)
-            c = eng.counts(slot)
-            for f in range(F):
-                import ctypes
-                found = ctypes.c_size_t(0)
-                _lib.raise_for(_lib.lib.sf_engine_signal(eng._h, slot, f, sig_buf.ctypes.data,
-                                                         len(sig_buf), ctypes.byref(found)),
-                               "signal")
-            d2h = int(c.sum()) * 16 + 4 * F
+            spots = eng.spots()
+            pixels = eng.pixels()
+            d2h = spots.nbytes + pixels.nbytes
         e2e_step(0)
         eng.synchronize()
         ranks.barrier()
@@ -358,18 +374,25 @@ def run_ours(args, ranks):
                "sample": f"{n} frames of 4362x4148, threshold on {threads} threads "
                          "and 3D grouping on one, as the reference CLI runs them"}
 
-    launches_per_step = 4  # threshold + placement reduce, scan, copy
+    # threshold; placement reduce, scan, copy; grouping: setup, gather, link,
+    # flatten, mark, 3 x scan (3 launches each), rank, scatter, accept, write,
+    # open, carry, finalize
+    launches_per_step = 1 + 3 + (5 + 4 * 3 + 7)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ranks.world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "u16 pixels, u32 sums, f32 tests", "data": "synthetic",
+        "dtype": "u16 pixels, u32 sums, f32 tests, f64 spots", "data": "synthetic",
         "config": {"workload": "Eiger2-16M-shaped uint16 frames, 4362x4148, batched engine",
                    "frames_per_step": F, "slots": 2, "distinct_frames": len(pool),
-                   "pipeline": "threshold + ordered compaction (grouping not yet in the timed step)",
+                   "pipeline": "threshold + ordered compaction + 3D grouping + spot pass",
                    "l2": "inputs larger than L2 (580 MB per step)",
                    "parallelism": f"replicas x{ranks.world}",
                    "engine": info},
+        "graph_replay": {"value": frames_total / (graph_ms / 1000.0), "unit": UNIT,
+                         "ms_per_step": graph_ms / args.steps},
+        "grouping": {"spots_per_frame": group_counts["accepted"] / max(1, F * (args.steps + args.warmup + 2)),
+                     "counts": group_counts, "live": live},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
                      "kernel": "threshold_kernel<uint16_t>",
@@ -377,7 +400,8 @@ def run_ours(args, ranks):
                      "algorithmic_bytes_per_launch": alg_bytes,
                      "traffic": (traffic * F if traffic else None)},
         "stage_ms_per_step": {"threshold": thr_ms,
-                              "placement": stage["place_ms"] / max(stage["runs"], 1)},
+                              "placement": stage["place_ms"] / max(stage["runs"], 1),
+                              "grouping": stage["group_ms"] / max(stage["runs"], 1)},
         "signal_pixels_per_frame": statistics.mean(nsig_per_step) / F,
         "clocks": clocks.summary(),
         "gpu_launches": launches_per_step * args.steps,

@@ -77,6 +77,16 @@ SIGNATURES = {
     "sf_profile_stages": (None, [_I]),
     "sf_profile_stages_enabled": (_I, []),
     "sf_last_stage_times": (None, [_P]),
+    "sf_labeller_create": (_I, [_S, _S, _P, ctypes.POINTER(_P)]),
+    "sf_labeller_destroy": (None, [_P]),
+    "sf_labeller_add": (_I, [_P, ctypes.c_int64, _P, _S]),
+    "sf_labeller_finish": (_I, [_P]),
+    "sf_labeller_counts": (_I, [_P, _P]),
+    "sf_labeller_nspots": (_S, [_P]),
+    "sf_labeller_npixels": (_S, [_P]),
+    "sf_labeller_live": (_S, [_P]),
+    "sf_labeller_spots": (_I, [_P, _P, _S]),
+    "sf_labeller_pixels": (_I, [_P, _P, _S]),
     "sf_engine_create": (_I, [_I, _I, _P, _P, _P, ctypes.POINTER(_P)]),
     "sf_engine_destroy": (None, [_P]),
     "sf_engine_info": (_I, [_P, _P]),
@@ -91,6 +101,11 @@ SIGNATURES = {
     "sf_engine_elapsed": (_I, [_P, _I, _I, ctypes.POINTER(ctypes.c_float)]),
     "sf_engine_profile": (_I, [_P, _I]),
     "sf_engine_stage_totals": (_I, [_P, _P]),
+    "sf_engine_enable_grouping": (_I, [_P, _P, ctypes.c_int64, ctypes.c_uint64]),
+    "sf_engine_group_counts": (_I, [_P, _P, ctypes.POINTER(ctypes.c_uint64)]),
+    "sf_engine_spots": (_I, [_P, _P, _S, ctypes.POINTER(_S)]),
+    "sf_engine_pixels": (_I, [_P, _P, _S, ctypes.POINTER(_S)]),
+    "sf_engine_finish": (_I, [_P]),
 }
 
 

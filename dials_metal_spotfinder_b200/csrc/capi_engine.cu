@@ -8,18 +8,21 @@
 // per slot orders "frames uploaded" before "run" and "run finished" before
 // the next upload into the same slot.
 
+#include <algorithm>
 #include <memory>
 #include <vector>
 
 #include "../../include/spotfinder_b200.h"
 #include "sf_capi.hh"
 #include "sf_host.hh"
+#include "sf_label.hh"
 
 namespace sf {
 namespace {
 
 constexpr int kMarks = 16;
 constexpr int kRingRuns = 4096;
+constexpr int kRunEvents = 4;
 
 } // namespace
 
@@ -27,15 +30,24 @@ struct Engine {
   std::unique_ptr<ThresholdPlan> plan;
   cudaStream_t compute = nullptr, copy = nullptr;
   std::vector<cudaEvent_t> uploaded, consumed; // per slot
-  std::vector<cudaGraphExec_t> graphs;         // per slot, when in use
+  // Graphs per (slot, labeller parity): the labeller alternates between two
+  // live buffers, so a captured run is only valid for the parity it saw.
+  std::vector<cudaGraphExec_t> graphs;
   bool use_graph = false;
   cudaEvent_t marks[kMarks] = {};
   // Profiling: per run, events before the threshold, between threshold and
-  // placement, and after the placement.
+  // placement, after the placement and after the grouping.
   bool profiling = false;
   std::vector<cudaEvent_t> ring;
   int ring_used = 0;
   uint32_t *pinned = nullptr;
+  // Grouping, when enabled: the labeller and the device copies of each
+  // frame's list offset and capacity.
+  std::unique_ptr<DeviceLabeller> lab;
+  uint64_t *d_offs = nullptr;
+  uint32_t *d_caps = nullptr;
+  int parity = 0;
+  LabelScalars *host_sc = nullptr;
 
   ~Engine() {
     if (compute)
@@ -45,6 +57,11 @@ struct Engine {
     for (cudaGraphExec_t g : graphs)
       if (g)
         cudaGraphExecDestroy(g);
+    lab.reset();
+    cudaFree(d_offs);
+    cudaFree(d_caps);
+    if (host_sc)
+      cudaFreeHost(host_sc);
     for (cudaEvent_t e : uploaded)
       cudaEventDestroy(e);
     for (cudaEvent_t e : consumed)
@@ -72,16 +89,27 @@ struct Engine {
       throw std::out_of_range("frame out of range");
   }
 
-  void enqueue_run(int slot, cudaEvent_t a, cudaEvent_t b, cudaEvent_t c) {
+  // Threshold, placement and (when enabled) grouping of one slot.
+  void enqueue_body(int slot, cudaEvent_t b, cudaEvent_t c) {
+    plan->enqueue(slot, compute, b);
+    if (c)
+      check(cudaEventRecord(c, compute), "cudaEventRecord");
+    if (lab)
+      lab->enqueue(plan->nframes(), plan->out(slot), d_offs, plan->frame_count(slot), d_caps,
+                   false, compute);
+  }
+
+  void enqueue_run(int slot, cudaEvent_t a, cudaEvent_t b, cudaEvent_t c, cudaEvent_t d) {
     if (a)
       check(cudaEventRecord(a, compute), "cudaEventRecord");
     if (use_graph) {
-      if (!graphs[slot]) {
+      cudaGraphExec_t &exec = graphs[2 * slot + parity];
+      if (!exec) {
         cudaGraph_t g = nullptr;
         check(cudaStreamBeginCapture(compute, cudaStreamCaptureModeThreadLocal),
               "beginning graph capture");
         try {
-          plan->enqueue(slot, compute, nullptr);
+          enqueue_body(slot, nullptr, nullptr);
         } catch (...) {
           cudaStreamEndCapture(compute, &g);
           if (g)
@@ -89,34 +117,78 @@ struct Engine {
           throw;
         }
         check(cudaStreamEndCapture(compute, &g), "ending graph capture");
-        cudaGraphExec_t exec = nullptr;
         const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
         cudaGraphDestroy(g);
         check(e, "instantiating the graph");
-        graphs[slot] = exec;
+      } else if (lab) {
+        lab->note_replayed(); // the captured run flips the live buffers too
       }
-      check(cudaGraphLaunch(graphs[slot], compute), "launching the graph");
-      if (b)
-        check(cudaEventRecord(b, compute), "cudaEventRecord");
+      check(cudaGraphLaunch(exec, compute), "launching the graph");
     } else {
-      plan->enqueue(slot, compute, b);
+      enqueue_body(slot, b, c);
     }
-    if (c)
-      check(cudaEventRecord(c, compute), "cudaEventRecord");
+    if (d)
+      check(cudaEventRecord(d, compute), "cudaEventRecord");
+    if (lab)
+      parity ^= 1;
   }
 
   void run(int slot) {
     check_slot(slot);
     check(cudaStreamWaitEvent(compute, uploaded[slot], 0), "ordering after the upload");
-    cudaEvent_t a = nullptr, b = nullptr, c = nullptr;
+    cudaEvent_t a = nullptr, b = nullptr, c = nullptr, d = nullptr;
     if (profiling && ring_used < kRingRuns) {
-      a = ring[3 * ring_used];
-      b = ring[3 * ring_used + 1];
-      c = ring[3 * ring_used + 2];
+      cudaEvent_t *e = &ring[kRunEvents * ring_used];
+      a = e[0];
+      b = e[1];
+      c = e[2];
+      d = e[3];
       ring_used++;
     }
-    enqueue_run(slot, a, b, c);
+    enqueue_run(slot, a, b, c, d);
     check(cudaEventRecord(consumed[slot], compute), "cudaEventRecord");
+  }
+
+  void enable_grouping(const GroupOptions &opt, int64_t first_frame, uint64_t carry_cap) {
+    if (lab)
+      throw std::invalid_argument("grouping is already enabled");
+    const int nf = plan->nframes();
+    int32_t h = plan->shape(0).height, w = plan->shape(0).width;
+    for (int f = 1; f < nf; f++)
+      if (plan->shape(f).height != h || plan->shape(f).width != w)
+        throw std::invalid_argument("grouping needs frames of one shape");
+    std::vector<uint64_t> offs(nf);
+    std::vector<uint32_t> caps(nf);
+    uint64_t total = 0, biggest = 0;
+    for (int f = 0; f < nf; f++) {
+      offs[f] = plan->out_base(f);
+      caps[f] = plan->capacity(f);
+      total += caps[f];
+      biggest = std::max<uint64_t>(biggest, caps[f]);
+    }
+    check(cudaMalloc(&d_offs, nf * sizeof(uint64_t)), "cudaMalloc");
+    check(cudaMalloc(&d_caps, nf * sizeof(uint32_t)), "cudaMalloc");
+    check(cudaMemcpy(d_offs, offs.data(), nf * sizeof(uint64_t), cudaMemcpyHostToDevice), "copy");
+    check(cudaMemcpy(d_caps, caps.data(), nf * sizeof(uint32_t), cudaMemcpyHostToDevice), "copy");
+    check(cudaMallocHost(&host_sc, sizeof(LabelScalars)), "cudaMallocHost");
+    lab = std::make_unique<DeviceLabeller>(h, w, opt);
+    lab->reserve(total, nf, carry_cap ? carry_cap : 2 * biggest + (1u << 20));
+    lab->set_next_frame(first_frame, compute);
+    check(cudaStreamSynchronize(compute), "cudaStreamSynchronize");
+    parity = 0;
+  }
+
+  const LabelScalars &group_state() {
+    if (!lab)
+      throw std::invalid_argument("grouping is not enabled");
+    check(cudaMemcpyAsync(host_sc, lab->scalars(), sizeof(LabelScalars), cudaMemcpyDeviceToHost,
+                          compute),
+          "reading the grouping state");
+    check(cudaStreamSynchronize(compute), "cudaStreamSynchronize");
+    if (host_sc->status != kLabelOk)
+      throw DeviceError("grouping capacity exceeded (status " + std::to_string(host_sc->status) +
+                        ")");
+    return *host_sc;
   }
 
   void upload(int slot, int frame, const void *host) {
@@ -191,7 +263,7 @@ int sf_engine_create(int elem_bytes, int nframes, const int32_t *heights,
       sf::check(cudaEventRecord(u, e->copy), "event");
       sf::check(cudaEventRecord(c, e->compute), "event");
     }
-    e->graphs.assign(slots, nullptr);
+    e->graphs.assign(2 * slots, nullptr);
     for (cudaEvent_t &m : e->marks)
       sf::check(cudaEventCreate(&m), "event");
     sf::check(cudaMallocHost(&e->pinned, (nframes + 1) * sizeof(uint32_t)), "cudaMallocHost");
@@ -305,7 +377,10 @@ int sf_engine_use_graph(sf_engine *engine, int on) {
   return guarded([&] {
     if (!engine)
       return -1;
-    reinterpret_cast<Engine *>(engine)->use_graph = on != 0;
+    Engine *e = reinterpret_cast<Engine *>(engine);
+    if (on && e->profiling)
+      throw std::invalid_argument("stage profiling is on: turn it off before graph replay");
+    e->use_graph = on != 0;
     return 0;
   });
 }
@@ -337,10 +412,13 @@ int sf_engine_profile(sf_engine *engine, int on) {
       return -1;
     Engine *e = reinterpret_cast<Engine *>(engine);
     if (on && e->ring.empty()) {
-      e->ring.resize(3 * sf::kRingRuns);
+      e->ring.resize(sf::kRunEvents * sf::kRingRuns);
       for (cudaEvent_t &ev : e->ring)
         sf::check(cudaEventCreate(&ev), "event");
     }
+    if (on && e->use_graph)
+      throw std::invalid_argument("stage profiling times the launches one by one: "
+                                  "turn graph replay off first");
     e->profiling = on != 0;
     e->ring_used = 0;
     return 0;
@@ -352,19 +430,104 @@ int sf_engine_stage_totals(sf_engine *engine, double *out4) {
     if (!engine || !out4)
       return -1;
     Engine *e = reinterpret_cast<Engine *>(engine);
-    double thr = 0, place = 0;
+    double thr = 0, place = 0, group = 0;
     for (int i = 0; i < e->ring_used; i++) {
-      float a = 0, b = 0;
-      sf::check(cudaEventSynchronize(e->ring[3 * i + 2]), "cudaEventSynchronize");
-      sf::check(cudaEventElapsedTime(&a, e->ring[3 * i], e->ring[3 * i + 1]), "elapsed");
-      sf::check(cudaEventElapsedTime(&b, e->ring[3 * i + 1], e->ring[3 * i + 2]), "elapsed");
+      cudaEvent_t *ev = &e->ring[sf::kRunEvents * i];
+      float a = 0, b = 0, c = 0;
+      sf::check(cudaEventSynchronize(ev[3]), "cudaEventSynchronize");
+      sf::check(cudaEventElapsedTime(&a, ev[0], ev[1]), "elapsed");
+      sf::check(cudaEventElapsedTime(&b, ev[1], ev[2]), "elapsed");
+      sf::check(cudaEventElapsedTime(&c, ev[2], ev[3]), "elapsed");
       thr += a;
       place += b;
+      group += c;
     }
     out4[0] = e->ring_used;
     out4[1] = thr;
     out4[2] = place;
-    out4[3] = 0.0;
+    out4[3] = group;
+    return 0;
+  });
+}
+
+int sf_engine_enable_grouping(sf_engine *engine, const sf_group_options *options,
+                              int64_t first_frame, uint64_t carry_capacity) {
+  return guarded([&] {
+    if (!engine)
+      return -1;
+    sf::GroupOptions opt;
+    if (options) {
+      opt.min_spot_size = options->min_spot_size;
+      opt.max_spot_size = options->max_spot_size;
+      opt.max_separation = options->max_separation;
+      opt.two_d = options->two_d != 0;
+    }
+    reinterpret_cast<Engine *>(engine)->enable_grouping(opt, first_frame, carry_capacity);
+    return 0;
+  });
+}
+
+int sf_engine_group_counts(sf_engine *engine, sf_counts *out, uint64_t *live) {
+  return guarded([&] {
+    if (!engine || !out)
+      return -1;
+    const sf::LabelScalars &s = reinterpret_cast<Engine *>(engine)->group_state();
+    out->signal_pixels = s.signal_pixels;
+    out->groups = s.groups;
+    out->too_small = s.too_small;
+    out->too_large = s.too_large;
+    out->separated = s.separated;
+    out->accepted = s.accepted;
+    if (live)
+      *live = s.carry_n;
+    return 0;
+  });
+}
+
+int sf_engine_spots(sf_engine *engine, sf_spot *out, size_t capacity, size_t *n) {
+  return guarded([&] {
+    if (!engine || !n)
+      return -1;
+    Engine *e = reinterpret_cast<Engine *>(engine);
+    const sf::LabelScalars &s = e->group_state();
+    *n = s.batch_spots;
+    if (s.batch_spots > capacity)
+      return -2;
+    if (s.batch_spots)
+      sf::check(cudaMemcpy(out, e->lab->batch_spots(), s.batch_spots * sizeof(sf::Spot),
+                           cudaMemcpyDeviceToHost),
+                "reading spots");
+    return 0;
+  });
+}
+
+int sf_engine_pixels(sf_engine *engine, sf_pixel *out, size_t capacity, size_t *n) {
+  return guarded([&] {
+    if (!engine || !n)
+      return -1;
+    Engine *e = reinterpret_cast<Engine *>(engine);
+    const sf::LabelScalars &s = e->group_state();
+    *n = s.batch_pixels;
+    if (s.batch_pixels > capacity)
+      return -2;
+    if (s.batch_pixels)
+      sf::check(cudaMemcpy(out, e->lab->batch_pixels(), s.batch_pixels * sizeof(sf::Pixel),
+                           cudaMemcpyDeviceToHost),
+                "reading spot pixels");
+    return 0;
+  });
+}
+
+int sf_engine_finish(sf_engine *engine) {
+  return guarded([&] {
+    if (!engine)
+      return -1;
+    Engine *e = reinterpret_cast<Engine *>(engine);
+    if (!e->lab)
+      throw std::invalid_argument("grouping is not enabled");
+    e->lab->enqueue(0, e->plan->out(0), e->d_offs, e->plan->frame_count(0), e->d_caps, true,
+                    e->compute);
+    e->parity ^= 1;
     return 0;
   });
 }

@@ -1,0 +1,753 @@
+// 3D / 2D six-connected grouping and the spot pass on the device, with the
+// streaming semantics of the reference's Labeller (src/dials_spots.cc:
+// 57-219) and its per-component arithmetic (src/dials_spots.cc:221-360).
+//
+// One batch (enqueue) is a fixed sequence of launches whose sizes all live
+// in device memory, so a batch can follow the threshold on the same stream
+// and be captured in the same CUDA graph:
+//
+//   setup     frame segments of the live set: the carry's last frame, then
+//             the batch frames; live size n
+//   gather    the batch's signal lists appended after the carried pixels,
+//             so the live set is in (frame, index) order; per-root fields
+//             cleared
+//   link      left, up and previous-frame neighbours joined by a lock-free
+//             union-find that links toward the lower position, so a root is
+//             its component's first pixel in (frame, index) order
+//   flatten   root of every pixel; component size and last frame
+//   mark      finished roots (no pixel on the batch's last frame) as one
+//             bitmap per last-frame bucket, with per-word counts
+//   scan      of the counts, bucket-major: the reference's emission order
+//             is (last frame, first pixel), which is exactly bucket then
+//             position
+//   rank      each finished component's emission rank; size filters
+//   scan      member offsets of the components that pass the size filters
+//   scatter   members, in any order
+//   accept    per component: members sorted by position (so (frame, index)
+//             order), then the FP64 pass in that order, peak-centroid
+//             filter
+//   scan      output rows and pixel offsets of the accepted spots
+//   write     spots and their pixels
+//   open/scan/carry  the open components' pixels compacted, in order, into
+//             the other live buffer and re-rooted at their first pixel
+//   finalize  running counts and the carry for the next batch
+//
+// Every loop here walks a bounded range; union-find paths strictly decrease
+// in position, so no loop depends on another thread making progress.
+
+#include <climits>
+
+#include "sf_label.hh"
+
+namespace sf {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr uint32_t kNone = 0xffffffffu;
+constexpr int kThreads = 256;
+
+struct LabArgs {
+  int32_t width;
+  int32_t nframes;
+  int32_t close_all;
+  int32_t two_d;
+  uint64_t min_size, max_size;
+  double max_sep;
+  uint64_t live_cap, spot_cap;
+  const SignalPixel *lists;
+  const uint64_t *offs;
+  const uint32_t *counts;
+  const uint32_t *caps;
+  int32_t *fr;
+  uint32_t *ix, *val, *par;
+  int32_t *nfr;
+  uint32_t *nix, *nval, *npar;
+  uint32_t *root, *size;
+  int32_t *lastz;
+  uint32_t *rank_of_root, *cursor;
+  uint32_t *bits, *bcnt;
+  uint32_t *comp_root, *msize, *moff, *members;
+  uint64_t *pack;
+  uint32_t *open;
+  Spot *spots;
+  Pixel *kept;
+  uint64_t *seg_start, *seg_count;
+  int64_t *seg_z;
+  LabelScalars *sc;
+};
+
+__device__ __forceinline__ uint64_t gtid() {
+  return static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+}
+__device__ __forceinline__ uint64_t gstride() {
+  return static_cast<uint64_t>(gridDim.x) * blockDim.x;
+}
+
+// Union-find on positions. Parents only ever point to lower positions.
+__device__ __forceinline__ uint32_t uf_find(uint32_t *parent, uint32_t x) {
+  volatile uint32_t *p = parent;
+  while (true) {
+    const uint32_t px = p[x];
+    if (px == x)
+      return x;
+    const uint32_t gp = p[px];
+    if (gp != px)
+      p[x] = gp; // path halving: still an ancestor, still lower
+    x = px;
+  }
+}
+
+__device__ __forceinline__ void uf_unite(uint32_t *parent, uint32_t a, uint32_t b) {
+  while (true) {
+    a = uf_find(parent, a);
+    b = uf_find(parent, b);
+    if (a == b)
+      return;
+    if (a < b) {
+      const uint32_t t = a;
+      a = b;
+      b = t;
+    }
+    // Link the higher root under the lower one, if it is still a root.
+    const uint32_t old = atomicCAS(&parent[a], a, b);
+    if (old == a)
+      return;
+    a = old;
+  }
+}
+
+// First position in [lo, hi) whose index is >= target.
+__device__ __forceinline__ uint64_t lower_bound(const uint32_t *ix, uint64_t lo, uint64_t hi,
+                                                uint32_t target) {
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if (ix[mid] < target)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ int segment_of(const uint64_t *seg_start, int nseg, uint64_t g) {
+  int lo = 0, hi = nseg - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (seg_start[mid] <= g)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ int bucket_of(const int64_t *seg_z, int nseg, int64_t z) {
+  int lo = 0, hi = nseg - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (seg_z[mid] <= z)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ int64_t last_batch_frame(const LabArgs &a) {
+  return a.sc->batch_z0 + a.nframes - 1;
+}
+
+// A root whose component is finished by this batch.
+__device__ __forceinline__ bool finished_root(const LabArgs &a, uint64_t g, uint64_t n) {
+  if (g >= n || a.root[g] != g)
+    return false;
+  if (a.close_all || a.two_d || a.nframes == 0)
+    return true;
+  return static_cast<int64_t>(a.lastz[g]) < last_batch_frame(a);
+}
+
+// --------------------------------------------------------------------------
+
+__global__ void lab_setup(LabArgs a) {
+  if (threadIdx.x != 0 || blockIdx.x != 0)
+    return;
+  LabelScalars *sc = a.sc;
+  const uint64_t carry = sc->carry_n;
+  int nseg = 0;
+  if (carry > 0) {
+    a.seg_z[0] = sc->carry_last_z;
+    a.seg_start[0] = sc->carry_last_start;
+    a.seg_count[0] = carry - sc->carry_last_start;
+    nseg = 1;
+  }
+  uint64_t pos = carry;
+  for (int f = 0; f < a.nframes; f++) {
+    uint32_t c = a.counts[f];
+    if (c > a.caps[f]) // an over-dense frame: its list holds only this many
+      c = a.caps[f];
+    if (pos + c > a.live_cap) {
+      sc->status = kLabelLiveOverflow;
+      c = static_cast<uint32_t>(a.live_cap - pos);
+    }
+    a.seg_z[nseg] = sc->batch_z0 + f;
+    a.seg_start[nseg] = pos;
+    a.seg_count[nseg] = c;
+    pos += c;
+    nseg++;
+  }
+  if (nseg == 0) { // nothing held and nothing added: one empty segment
+    a.seg_z[0] = sc->batch_z0;
+    a.seg_start[0] = 0;
+    a.seg_count[0] = 0;
+    nseg = 1;
+  }
+  sc->n = pos;
+  sc->nw = (pos + 31) / 32;
+  sc->nseg = nseg;
+  sc->seg_len = static_cast<uint64_t>(nseg) * sc->nw;
+  sc->signal_pixels += pos - carry;
+  sc->next_carry_last_start = ~0ull;
+  sc->closed32 = sc->members32 = sc->open32 = 0;
+  sc->accepted_pack = 0;
+}
+
+__global__ void __launch_bounds__(kThreads) lab_gather(LabArgs a) {
+  const LabelScalars *sc = a.sc;
+  const uint64_t n = sc->n, carry = sc->carry_n;
+  const int nseg = static_cast<int>(sc->nseg);
+  const int first_batch_seg = carry > 0 ? 1 : 0;
+  for (uint64_t g = gtid(); g < n; g += gstride()) {
+    a.size[g] = 0;
+    a.lastz[g] = INT_MIN;
+    a.rank_of_root[g] = kNone;
+    a.cursor[g] = 0;
+    if (g >= carry) {
+      const int s = segment_of(a.seg_start, nseg, g);
+      const int f = s - first_batch_seg;
+      const SignalPixel px = a.lists[a.offs[f] + (g - a.seg_start[s])];
+      a.fr[g] = static_cast<int32_t>(a.seg_z[s]);
+      a.ix[g] = px.index;
+      a.val[g] = px.value;
+      a.par[g] = static_cast<uint32_t>(g);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) lab_link(LabArgs a) {
+  const LabelScalars *sc = a.sc;
+  const uint64_t n = sc->n, carry = sc->carry_n;
+  const int nseg = static_cast<int>(sc->nseg);
+  const uint32_t W = static_cast<uint32_t>(a.width);
+  for (uint64_t g = carry + gtid(); g < n; g += gstride()) {
+    const int s = segment_of(a.seg_start, nseg, g);
+    const uint64_t s0 = a.seg_start[s];
+    const uint32_t idx = a.ix[g];
+    // the pixel to the left, in the same row (src/dials_spots.cc:106-110)
+    if (g > s0 && idx % W != 0 && a.ix[g - 1] + 1 == idx)
+      uf_unite(a.par, static_cast<uint32_t>(g), static_cast<uint32_t>(g - 1));
+    // the pixel above (src/dials_spots.cc:115-123)
+    if (idx >= W) {
+      const uint64_t j = lower_bound(a.ix, s0, g, idx - W);
+      if (j < g && a.ix[j] == idx - W)
+        uf_unite(a.par, static_cast<uint32_t>(g), static_cast<uint32_t>(j));
+    }
+    // the same pixel on the previous frame, if it is the frame before
+    // (src/dials_spots.cc:128-137)
+    if (!a.two_d && s > 0 && a.seg_z[s - 1] + 1 == a.seg_z[s]) {
+      const uint64_t p0 = a.seg_start[s - 1], p1 = p0 + a.seg_count[s - 1];
+      const uint64_t j = lower_bound(a.ix, p0, p1, idx);
+      if (j < p1 && a.ix[j] == idx)
+        uf_unite(a.par, static_cast<uint32_t>(g), static_cast<uint32_t>(j));
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) lab_flatten(LabArgs a) {
+  const uint64_t n = a.sc->n;
+  for (uint64_t g = gtid(); g < n; g += gstride()) {
+    const uint32_t r = uf_find(a.par, static_cast<uint32_t>(g));
+    a.root[g] = r;
+    atomicAdd(&a.size[r], 1u);
+    atomicMax(&a.lastz[r], a.fr[g]);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) lab_mark(LabArgs a) {
+  const LabelScalars *sc = a.sc;
+  const uint64_t n = sc->n, nw = sc->nw;
+  const int nseg = static_cast<int>(sc->nseg);
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = gtid() >> 5, nwarps = gstride() >> 5;
+  for (uint64_t w = warp; w < nw; w += nwarps) {
+    const uint64_t g = w * 32 + lane;
+    const bool fin = finished_root(a, g, n);
+    const int b = fin ? bucket_of(a.seg_z, nseg, a.lastz[g]) : -1;
+    for (int s = 0; s < nseg; s++) {
+      const uint32_t m = __ballot_sync(kFull, b == s);
+      if (lane == 0) {
+        a.bits[s * nw + w] = m;
+        a.bcnt[s * nw + w] = __popc(m);
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) lab_rank(LabArgs a) {
+  LabelScalars *sc = a.sc;
+  const uint64_t n = sc->n, nw = sc->nw;
+  const int nseg = static_cast<int>(sc->nseg);
+  if (gtid() == 0)
+    sc->closed = sc->closed32;
+  uint32_t small = 0, large = 0;
+  for (uint64_t g = gtid(); g < n; g += gstride()) {
+    if (!finished_root(a, g, n))
+      continue;
+    const int b = bucket_of(a.seg_z, nseg, a.lastz[g]);
+    const uint64_t w = g >> 5;
+    const uint32_t lane_mask = (1u << (g & 31)) - 1u;
+    const uint32_t rank = a.bcnt[b * nw + w] + __popc(a.bits[b * nw + w] & lane_mask);
+    a.rank_of_root[g] = rank;
+    a.comp_root[rank] = static_cast<uint32_t>(g);
+    const uint32_t size = a.size[g];
+    const bool keep = size >= a.min_size && size <= a.max_size;
+    a.msize[rank] = keep ? size : 0u;
+    small += size < a.min_size;
+    large += size > a.max_size;
+  }
+  if (small)
+    atomicAdd(reinterpret_cast<unsigned long long *>(&sc->too_small), small);
+  if (large)
+    atomicAdd(reinterpret_cast<unsigned long long *>(&sc->too_large), large);
+}
+
+__global__ void __launch_bounds__(kThreads) lab_scatter(LabArgs a) {
+  const uint64_t n = a.sc->n;
+  for (uint64_t g = gtid(); g < n; g += gstride()) {
+    const uint32_t r = a.root[g];
+    const uint32_t rank = a.rank_of_root[r];
+    if (rank == kNone || a.msize[rank] == 0)
+      continue;
+    const uint32_t at = atomicAdd(&a.cursor[r], 1u);
+    a.members[a.moff[rank] + at] = static_cast<uint32_t>(g);
+  }
+}
+
+// Shell sort of a short array (a spot has at most max_spot_size members).
+__device__ void sort_positions(uint32_t *v, uint32_t n) {
+  const uint32_t gaps[] = {701, 301, 132, 57, 23, 10, 4, 1};
+  for (uint32_t gap : gaps) {
+    if (gap >= n)
+      continue;
+    for (uint32_t i = gap; i < n; i++) {
+      const uint32_t t = v[i];
+      uint32_t j = i;
+      while (j >= gap && v[j - gap] > t) {
+        v[j] = v[j - gap];
+        j -= gap;
+      }
+      v[j] = t;
+    }
+  }
+}
+
+// The per-component arithmetic of src/dials_spots.cc:221-360, in the
+// reference's order, one IEEE rounding per operation (explicit _rn so that
+// nothing is fused). Returns whether the spot passes the peak-centroid
+// filter; fills *spot either way.
+__device__ bool spot_pass(const LabArgs &a, const uint32_t *m, uint32_t n, Spot *spot) {
+  const uint32_t W = static_cast<uint32_t>(a.width);
+  const double pixel_variance = 1.0 / 12.0;
+  double sum = 0.0, sum_sq = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
+  int32_t x0 = 0, x1 = 0, y0 = 0, y1 = 0, z0 = 0, z1 = 0;
+  uint32_t peak_value = 0;
+  double px = 0.0, py = 0.0, pz = 0.0;
+  for (uint32_t k = 0; k < n; k++) {
+    const uint32_t g = m[k];
+    const uint32_t idx = a.ix[g];
+    const int32_t x = static_cast<int32_t>(idx % W);
+    const int32_t y = static_cast<int32_t>(idx / W);
+    const int32_t z = a.fr[g];
+    if (k == 0) {
+      x0 = x; x1 = x + 1; y0 = y; y1 = y + 1; z0 = z; z1 = z + 1;
+    } else {
+      x0 = min(x0, x); x1 = max(x1, x + 1);
+      y0 = min(y0, y); y1 = max(y1, y + 1);
+      z0 = min(z0, z); z1 = max(z1, z + 1);
+    }
+    const uint32_t v = a.val[g];
+    const double value = __uint2double_rn(v);
+    const double cx = __dadd_rn(__int2double_rn(x), 0.5);
+    const double cy = __dadd_rn(__int2double_rn(y), 0.5);
+    const double cz = __dadd_rn(__int2double_rn(z), 0.5);
+    sum = __dadd_rn(sum, value);
+    sum_sq = __dadd_rn(sum_sq, __dmul_rn(value, value));
+    wx = __dadd_rn(wx, __dmul_rn(value, cx));
+    wy = __dadd_rn(wy, __dmul_rn(value, cy));
+    wz = __dadd_rn(wz, __dmul_rn(value, cz));
+    if (v > peak_value) {
+      peak_value = v;
+      px = cx; py = cy; pz = cz;
+    }
+  }
+  spot->bbox[0] = x0; spot->bbox[1] = x1;
+  spot->bbox[2] = y0; spot->bbox[3] = y1;
+  spot->bbox[4] = z0; spot->bbox[5] = z1;
+  spot->intensity = sum;
+  spot->intensity_variance = sum;
+  spot->n_signal = n;
+  if (sum > 0.0) {
+    const double mx = __ddiv_rn(wx, sum), my = __ddiv_rn(wy, sum);
+    double mz = __ddiv_rn(wz, sum);
+    double dx2 = 0.0, dy2 = 0.0, dz2 = 0.0;
+    for (uint32_t k = 0; k < n; k++) {
+      const uint32_t g = m[k];
+      const uint32_t idx = a.ix[g];
+      const double value = __uint2double_rn(a.val[g]);
+      const double dx = __dsub_rn(__dadd_rn(__uint2double_rn(idx % W), 0.5), mx);
+      const double dy = __dsub_rn(__dadd_rn(__uint2double_rn(idx / W), 0.5), my);
+      const double dz = __dsub_rn(__dadd_rn(__int2double_rn(a.fr[g]), 0.5), mz);
+      dx2 = __dadd_rn(dx2, __dmul_rn(__dmul_rn(value, dx), dx));
+      dy2 = __dadd_rn(dy2, __dmul_rn(__dmul_rn(value, dy), dy));
+      dz2 = __dadd_rn(dz2, __dmul_rn(__dmul_rn(value, dz), dz));
+    }
+    const double ss = __dmul_rn(sum, sum);
+    if (ss > sum_sq) {
+      const double den = __dsub_rn(ss, sum_sq);
+      spot->variance[0] = __dadd_rn(__ddiv_rn(__ddiv_rn(__dmul_rn(dx2, sum), den), sum), pixel_variance);
+      spot->variance[1] = __dadd_rn(__ddiv_rn(__ddiv_rn(__dmul_rn(dy2, sum), den), sum), pixel_variance);
+      spot->variance[2] = __dadd_rn(__ddiv_rn(__ddiv_rn(__dmul_rn(dz2, sum), den), sum), pixel_variance);
+    } else {
+      spot->variance[0] = spot->variance[1] = spot->variance[2] = pixel_variance;
+    }
+    if (z1 == z0 + 1)
+      mz = __dadd_rn(__int2double_rn(z0), 0.5);
+    spot->position[0] = mx;
+    spot->position[1] = my;
+    spot->position[2] = mz;
+  } else {
+    spot->variance[0] = spot->variance[1] = spot->variance[2] = 0.0;
+    spot->position[0] = __ddiv_rn(__int2double_rn(x1 + x0), 2.0);
+    spot->position[1] = __ddiv_rn(__int2double_rn(y1 + y0), 2.0);
+    spot->position[2] = __ddiv_rn(__int2double_rn(z1 + z0), 2.0);
+  }
+  if (a.max_sep > 0.0) {
+    const double dx = __dsub_rn(px, spot->position[0]);
+    const double dy = __dsub_rn(py, spot->position[1]);
+    const double dz = __dsub_rn(pz, spot->position[2]);
+    const double d = __dsqrt_rn(
+        __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+    if (d > a.max_sep)
+      return false;
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(kThreads) lab_accept(LabArgs a) {
+  LabelScalars *sc = a.sc;
+  const uint64_t closed = sc->closed;
+  uint32_t separated = 0;
+  for (uint64_t r = gtid(); r < closed; r += gstride()) {
+    const uint32_t n = a.msize[r];
+    if (n == 0) {
+      a.pack[r] = 0;
+      continue;
+    }
+    uint32_t *m = a.members + a.moff[r];
+    sort_positions(m, n);
+    Spot spot{}; // zeroed, padding included, so rows compare byte for byte
+    const bool ok = spot_pass(a, m, n, &spot);
+    if (!ok) {
+      separated++;
+      a.msize[r] = 0;
+      a.pack[r] = 0;
+    } else {
+      a.pack[r] = (static_cast<uint64_t>(n) << 32) | 1u;
+    }
+  }
+  if (separated)
+    atomicAdd(reinterpret_cast<unsigned long long *>(&sc->separated), separated);
+}
+
+__global__ void __launch_bounds__(kThreads) lab_write(LabArgs a) {
+  LabelScalars *sc = a.sc;
+  const uint64_t closed = sc->closed;
+  const uint64_t kept_base = sc->kept_total;
+  for (uint64_t r = gtid(); r < closed; r += gstride()) {
+    const uint32_t n = a.msize[r];
+    if (n == 0)
+      continue;
+    const uint64_t row = a.pack[r] & 0xffffffffu;
+    const uint64_t pix = a.pack[r] >> 32;
+    const uint32_t *m = a.members + a.moff[r];
+    Spot spot{}; // zeroed, padding included, so rows compare byte for byte
+    spot_pass(a, m, n, &spot);
+    spot.first = kept_base + pix;
+    if (row >= a.spot_cap || pix + n > a.live_cap) {
+      sc->status = kLabelSpotOverflow;
+      continue;
+    }
+    a.spots[row] = spot;
+    for (uint32_t k = 0; k < n; k++) {
+      const uint32_t g = m[k];
+      Pixel p;
+      p.frame = a.fr[g];
+      p.index = a.ix[g];
+      p.value = a.val[g];
+      a.kept[pix + k] = p;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) lab_open(LabArgs a) {
+  const uint64_t n = a.sc->n;
+  for (uint64_t g = gtid(); g < n; g += gstride())
+    a.open[g] = a.rank_of_root[a.root[g]] == kNone ? 1u : 0u;
+}
+
+__global__ void __launch_bounds__(kThreads) lab_carry(LabArgs a) {
+  LabelScalars *sc = a.sc;
+  const uint64_t n = sc->n;
+  const int64_t zlast = last_batch_frame(a);
+  for (uint64_t g = gtid(); g < n; g += gstride()) {
+    const uint32_t r = a.root[g];
+    if (a.rank_of_root[r] != kNone)
+      continue;
+    const uint32_t at = a.open[g]; // exclusive scan of the open flags
+    a.nfr[at] = a.fr[g];
+    a.nix[at] = a.ix[g];
+    a.nval[at] = a.val[g];
+    a.npar[at] = a.open[r]; // the root is open too, and comes first
+    if (static_cast<int64_t>(a.fr[g]) == zlast)
+      atomicMin(reinterpret_cast<unsigned long long *>(&sc->next_carry_last_start),
+                static_cast<unsigned long long>(at));
+  }
+}
+
+__global__ void lab_finalize(LabArgs a) {
+  if (threadIdx.x != 0 || blockIdx.x != 0)
+    return;
+  LabelScalars *sc = a.sc;
+  const bool all = a.close_all || a.two_d || a.nframes == 0;
+  sc->groups += sc->closed;
+  const uint64_t rows = sc->accepted_pack & 0xffffffffu;
+  const uint64_t pixels = sc->accepted_pack >> 32;
+  sc->accepted += rows;
+  sc->kept_total += pixels;
+  sc->batch_spots = rows;
+  sc->batch_pixels = pixels;
+  sc->carry_n = all ? 0 : sc->open32;
+  sc->carry_last_z = last_batch_frame(a);
+  sc->carry_last_start = sc->carry_n > 0 ? sc->next_carry_last_start : 0;
+  sc->batch_z0 += a.nframes;
+}
+
+} // namespace
+
+// --------------------------------------------------------------------------
+
+DeviceLabeller::DeviceLabeller(int height, int width, const GroupOptions &options)
+    : height_(height), width_(width), opt_(options) {
+  if (height < 1 || width < 1)
+    throw std::invalid_argument("dials_spots: a frame with no pixels in it");
+  if (opt_.max_spot_size < opt_.min_spot_size)
+    throw std::invalid_argument("dials_spots: max_spot_size is below min_spot_size");
+  if (opt_.min_spot_size == 0)
+    throw std::invalid_argument("dials_spots: min_spot_size must be at least 1");
+  if (static_cast<uint64_t>(height) * width > 0xffffffffull)
+    throw std::invalid_argument("dials_spots: frame too large");
+  check(cudaMalloc(&sc_, sizeof(LabelScalars)), "cudaMalloc labeller scalars");
+  check(cudaMemset(sc_, 0, sizeof(LabelScalars)), "clearing labeller scalars");
+  check(cudaMallocHost(&z_stage_, sizeof(int64_t)), "cudaMallocHost");
+  check(cudaStreamSynchronize(cudaStreamLegacy), "clearing labeller scalars");
+}
+
+DeviceLabeller::~DeviceLabeller() {
+  release();
+  cudaFree(sc_);
+  if (z_stage_)
+    cudaFreeHost(z_stage_);
+}
+
+void DeviceLabeller::release() {
+  for (Live &l : live_) {
+    cudaFree(l.frame);
+    cudaFree(l.index);
+    cudaFree(l.value);
+    cudaFree(l.parent);
+    l = Live();
+  }
+  void *ptrs[] = {root_, size_, rank_of_root_, cursor_, lastz_, bits_, bcnt_, comp_root_,
+                  msize_, moff_, members_, pack_, open_, spots_out_, kept_out_, seg_start_,
+                  seg_count_, seg_z_};
+  for (void *p : ptrs)
+    cudaFree(p);
+  root_ = size_ = rank_of_root_ = cursor_ = nullptr;
+  lastz_ = nullptr;
+  bits_ = bcnt_ = comp_root_ = msize_ = moff_ = members_ = open_ = nullptr;
+  pack_ = nullptr;
+  spots_out_ = nullptr;
+  kept_out_ = nullptr;
+  seg_start_ = seg_count_ = nullptr;
+  seg_z_ = nullptr;
+}
+
+void DeviceLabeller::reserve(uint64_t batch_pixels, int max_frames, uint64_t carry_pixels) {
+  if (batch_pixels <= batch_cap_ && max_frames <= frame_cap_ && carry_pixels <= carry_cap_)
+    return;
+  const uint64_t bc = std::max(batch_pixels, batch_cap_);
+  const int fc = std::max(max_frames, frame_cap_);
+  const uint64_t cc = std::max(carry_pixels, carry_cap_);
+  const uint64_t live = bc + cc;
+  if (live >= 0xffffffffull)
+    throw std::invalid_argument("labelling batch too large");
+  // Growing keeps the carry: copy it across after reallocating.
+  check(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
+  LabelScalars host;
+  check(cudaMemcpy(&host, sc_, sizeof(host), cudaMemcpyDeviceToHost), "reading scalars");
+  std::vector<int32_t> fr(host.carry_n);
+  std::vector<uint32_t> ix(host.carry_n), val(host.carry_n), par(host.carry_n);
+  if (host.carry_n) {
+    const Live &c = live_[cur_];
+    check(cudaMemcpy(fr.data(), c.frame, host.carry_n * 4, cudaMemcpyDeviceToHost), "carry");
+    check(cudaMemcpy(ix.data(), c.index, host.carry_n * 4, cudaMemcpyDeviceToHost), "carry");
+    check(cudaMemcpy(val.data(), c.value, host.carry_n * 4, cudaMemcpyDeviceToHost), "carry");
+    check(cudaMemcpy(par.data(), c.parent, host.carry_n * 4, cudaMemcpyDeviceToHost), "carry");
+  }
+  release();
+  const uint64_t nwmax = live / 32 + 1;
+  const uint64_t spot_cap = live / opt_.min_spot_size + 1;
+  try {
+    auto alloc = [](auto **p, uint64_t count, const char *what) {
+      check(cudaMalloc(reinterpret_cast<void **>(p), std::max<uint64_t>(count, 1) * sizeof(**p)),
+            what);
+    };
+    for (Live &l : live_) {
+      alloc(&l.frame, live, "live frames");
+      alloc(&l.index, live, "live indices");
+      alloc(&l.value, live, "live values");
+      alloc(&l.parent, live, "live parents");
+    }
+    alloc(&root_, live, "roots");
+    alloc(&size_, live, "sizes");
+    alloc(&rank_of_root_, live, "ranks");
+    alloc(&cursor_, live, "cursors");
+    alloc(&lastz_, live, "last frames");
+    alloc(&bits_, (fc + 1) * nwmax, "bucket bitmaps");
+    alloc(&bcnt_, (fc + 1) * nwmax, "bucket counts");
+    alloc(&comp_root_, live, "components");
+    alloc(&msize_, live, "member sizes");
+    alloc(&moff_, live, "member offsets");
+    alloc(&members_, live, "members");
+    alloc(&pack_, live, "spot offsets");
+    alloc(&open_, live, "open flags");
+    alloc(&spots_out_, spot_cap, "spots");
+    alloc(&kept_out_, live, "spot pixels");
+    alloc(&seg_start_, fc + 1, "segments");
+    alloc(&seg_count_, fc + 1, "segments");
+    alloc(&seg_z_, fc + 1, "segments");
+    scan32_.reserve((fc + 1) * nwmax);
+    scan32_.reserve(live);
+    scan64_.reserve(live);
+  } catch (...) {
+    release();
+    batch_cap_ = carry_cap_ = live_cap_ = spot_cap_ = 0;
+    frame_cap_ = 0;
+    throw;
+  }
+  if (host.carry_n) {
+    const Live &c = live_[cur_];
+    check(cudaMemcpy(c.frame, fr.data(), host.carry_n * 4, cudaMemcpyHostToDevice), "carry");
+    check(cudaMemcpy(c.index, ix.data(), host.carry_n * 4, cudaMemcpyHostToDevice), "carry");
+    check(cudaMemcpy(c.value, val.data(), host.carry_n * 4, cudaMemcpyHostToDevice), "carry");
+    check(cudaMemcpy(c.parent, par.data(), host.carry_n * 4, cudaMemcpyHostToDevice), "carry");
+  }
+  batch_cap_ = bc;
+  frame_cap_ = fc;
+  carry_cap_ = cc;
+  live_cap_ = live;
+  spot_cap_ = spot_cap;
+}
+
+void DeviceLabeller::set_next_frame(int64_t z, cudaStream_t s) {
+  check(cudaStreamSynchronize(s), "cudaStreamSynchronize"); // the staging word is reused
+  *z_stage_ = z;
+  check(cudaMemcpyAsync(&sc_->batch_z0, z_stage_, sizeof(int64_t), cudaMemcpyHostToDevice, s),
+        "setting the frame number");
+}
+
+void DeviceLabeller::enqueue(int nframes, const SignalPixel *lists, const uint64_t *offs,
+                             const uint32_t *counts, const uint32_t *caps, bool close_all,
+                             cudaStream_t s) {
+  if (nframes > frame_cap_)
+    throw std::invalid_argument("more frames than the labeller was sized for");
+  if (live_cap_ == 0)
+    throw std::invalid_argument("the labeller has no capacity: reserve() first");
+  LabArgs a;
+  a.width = width_;
+  a.nframes = nframes;
+  a.close_all = close_all ? 1 : 0;
+  a.two_d = opt_.two_d ? 1 : 0;
+  a.min_size = opt_.min_spot_size;
+  a.max_size = opt_.max_spot_size;
+  a.max_sep = opt_.max_separation;
+  a.live_cap = live_cap_;
+  a.spot_cap = spot_cap_;
+  a.lists = lists;
+  a.offs = offs;
+  a.counts = counts;
+  a.caps = caps;
+  const Live &cur = live_[cur_];
+  const Live &nxt = live_[cur_ ^ 1];
+  a.fr = cur.frame;
+  a.ix = cur.index;
+  a.val = cur.value;
+  a.par = cur.parent;
+  a.nfr = nxt.frame;
+  a.nix = nxt.index;
+  a.nval = nxt.value;
+  a.npar = nxt.parent;
+  a.root = root_;
+  a.size = size_;
+  a.lastz = lastz_;
+  a.rank_of_root = rank_of_root_;
+  a.cursor = cursor_;
+  a.bits = bits_;
+  a.bcnt = bcnt_;
+  a.comp_root = comp_root_;
+  a.msize = msize_;
+  a.moff = moff_;
+  a.members = members_;
+  a.pack = pack_;
+  a.open = open_;
+  a.spots = spots_out_;
+  a.kept = kept_out_;
+  a.seg_start = seg_start_;
+  a.seg_count = seg_count_;
+  a.seg_z = seg_z_;
+  a.sc = sc_;
+
+  const unsigned grid = static_cast<unsigned>(device_sm_count() * 8);
+  LabelScalars *sc = sc_;
+  lab_setup<<<1, 32, 0, s>>>(a);
+  lab_gather<<<grid, kThreads, 0, s>>>(a);
+  lab_link<<<grid, kThreads, 0, s>>>(a);
+  lab_flatten<<<grid, kThreads, 0, s>>>(a);
+  lab_mark<<<grid, kThreads, 0, s>>>(a);
+  const uint64_t nwmax = live_cap_ / 32 + 1;
+  scan32_.run(bcnt_, bcnt_, &sc->seg_len, 1, static_cast<uint64_t>(frame_cap_ + 1) * nwmax,
+              &sc->closed32, s);
+  lab_rank<<<grid, kThreads, 0, s>>>(a);
+  scan32_.run(msize_, moff_, &sc->closed, 1, live_cap_, &sc->members32, s);
+  lab_scatter<<<grid, kThreads, 0, s>>>(a);
+  lab_accept<<<grid, kThreads, 0, s>>>(a);
+  scan64_.run(pack_, pack_, &sc->closed, 1, live_cap_, &sc->accepted_pack, s);
+  lab_write<<<grid, kThreads, 0, s>>>(a);
+  lab_open<<<grid, kThreads, 0, s>>>(a);
+  scan32_.run(open_, open_, &sc->n, 1, live_cap_, &sc->open32, s);
+  lab_carry<<<grid, kThreads, 0, s>>>(a);
+  lab_finalize<<<1, 32, 0, s>>>(a);
+  check(cudaGetLastError(), "launching the labeller");
+  cur_ ^= 1;
+}
+
+} // namespace sf

@@ -9,7 +9,8 @@ import ctypes
 
 import numpy as np
 
-from ._lib import SIGNAL_PIXEL, EngineConfig, lib, raise_for, require_device
+from ._lib import (COUNT_NAMES, PIXEL, SIGNAL_PIXEL, SPOT, EngineConfig, GroupOptions, lib,
+                   raise_for, require_device)
 
 
 class Engine:
@@ -118,3 +119,43 @@ class Engine:
         raise_for(lib.sf_engine_stage_totals(self._h, out), "stage_totals")
         return {"runs": int(out[0]), "threshold_ms": out[1], "place_ms": out[2],
                 "group_ms": out[3]}
+
+    # -- grouping inside each run ------------------------------------------
+    def enable_grouping(self, first_frame: int = 0, min_spot_size=3, max_spot_size=1000,
+                        max_separation=2.0, two_d=False, carry_capacity=0) -> None:
+        """Every run's frames are the next consecutive frames of one series;
+        they are grouped on the device right after their threshold (the
+        reference's Labeller::add per frame, src/dials_spots.cc:57-145)."""
+        opt = GroupOptions(min_spot_size, max_spot_size, max_separation, int(two_d), 0)
+        raise_for(lib.sf_engine_enable_grouping(self._h, ctypes.byref(opt), int(first_frame),
+                                                int(carry_capacity)), "enable_grouping")
+
+    def group_counts(self):
+        out = (ctypes.c_uint64 * 6)()
+        live = ctypes.c_uint64(0)
+        raise_for(lib.sf_engine_group_counts(self._h, out, ctypes.byref(live)), "group_counts")
+        return dict(zip(COUNT_NAMES, (int(v) for v in out))), int(live.value)
+
+    def spots(self) -> np.ndarray:
+        """Spots finished by the last run (or by finish())."""
+        n = ctypes.c_size_t(0)
+        status = lib.sf_engine_spots(self._h, None, 0, ctypes.byref(n))
+        if status not in (0, -2):
+            raise_for(status, "spots")
+        out = np.zeros(n.value, SPOT)
+        raise_for(lib.sf_engine_spots(self._h, out.ctypes.data if n.value else None, n.value,
+                                      ctypes.byref(n)), "spots")
+        return out
+
+    def pixels(self) -> np.ndarray:
+        n = ctypes.c_size_t(0)
+        status = lib.sf_engine_pixels(self._h, None, 0, ctypes.byref(n))
+        if status not in (0, -2):
+            raise_for(status, "pixels")
+        out = np.zeros(n.value, PIXEL)
+        raise_for(lib.sf_engine_pixels(self._h, out.ctypes.data if n.value else None, n.value,
+                                       ctypes.byref(n)), "pixels")
+        return out
+
+    def finish(self) -> None:
+        raise_for(lib.sf_engine_finish(self._h), "finish")

@@ -122,6 +122,36 @@ SF_API void sf_profile_stages(int on);
 SF_API int sf_profile_stages_enabled(void);
 SF_API void sf_last_stage_times(double out6[6]);
 
+/* ---- grouping: src/dials_spots.hh:108-126 (dials_spots::Labeller) ------- *
+ *
+ * 3D (or, with two_d, per-frame) six-connected grouping of signal pixels on
+ * the device, and the centroid / variance / intensity / filter pass, with
+ * the reference's streaming semantics: frames in ascending order, a gap in
+ * the numbering closes everything open, spots come out ordered by the frame
+ * their component closed on and then by first pixel. Spots and pixels are
+ * byte-identical to the reference's (centroids and variances included: the
+ * double arithmetic runs in the reference's order). */
+typedef struct sf_labeller sf_labeller;
+
+SF_API int sf_labeller_create(size_t height, size_t width, const sf_group_options *options,
+                              sf_labeller **out);
+SF_API void sf_labeller_destroy(sf_labeller *labeller);
+/* Labeller::add: `signal` ascending by index (what the threshold emits).
+ * -4 (nothing changed) if the frame is not after the last one, a pixel is
+ * off the frame or the pixels are not ascending. */
+SF_API int sf_labeller_add(sf_labeller *labeller, int64_t frame, const sf_signal_pixel *signal,
+                           size_t n);
+/* Labeller::finish: close everything still open. */
+SF_API int sf_labeller_finish(sf_labeller *labeller);
+SF_API int sf_labeller_counts(sf_labeller *labeller, sf_counts *out);
+SF_API size_t sf_labeller_nspots(sf_labeller *labeller);
+SF_API size_t sf_labeller_npixels(sf_labeller *labeller);
+/* Labeller::live: pixels held for components that may still grow. */
+SF_API size_t sf_labeller_live(sf_labeller *labeller);
+/* Labeller::spots / pixels, copied out; -2 if `capacity` is too small. */
+SF_API int sf_labeller_spots(sf_labeller *labeller, sf_spot *out, size_t capacity);
+SF_API int sf_labeller_pixels(sf_labeller *labeller, sf_pixel *out, size_t capacity);
+
 /* ---- the batched engine ------------------------------------------------- *
  * No single reference counterpart: it replaces the reference's pattern of
  * -j host threads each calling gpu::find on one frame (src/find_spots.cc:
@@ -168,12 +198,30 @@ SF_API int sf_engine_signal(sf_engine *engine, int slot, int frame, sf_signal_pi
  * two marks (waits for the later one). */
 SF_API int sf_engine_record(sf_engine *engine, int mark);
 SF_API int sf_engine_elapsed(sf_engine *engine, int from, int to, float *ms);
-/* Per-run events around the threshold kernel and the placement (outside
- * graph replay they time each apart; inside it the two together). Turning
- * it on resets the totals; sf_engine_stage_totals gives runs, threshold ms,
- * placement ms, and 0, summed over the runs since. */
+/* Per-run events around the threshold kernel, the placement and the
+ * grouping (not with graph replay, which runs them as one). Turning it on
+ * resets the totals; sf_engine_stage_totals gives runs, threshold ms,
+ * placement ms and grouping ms, summed over the runs since. */
 SF_API int sf_engine_profile(sf_engine *engine, int on);
 SF_API int sf_engine_stage_totals(sf_engine *engine, double out4[4]);
+
+/* Grouping inside every run (frames of one shape): each run's frames are
+ * the next consecutive frames of one series starting at `first_frame`, and
+ * go through sf_labeller's arithmetic on the device right after their
+ * threshold, in the same stream (and graph). `carry_capacity` bounds the
+ * pixels held open between runs (0: twice a frame's list capacity plus
+ * 2^20); going past it makes the run report -3. */
+SF_API int sf_engine_enable_grouping(sf_engine *engine, const sf_group_options *options,
+                                     int64_t first_frame, uint64_t carry_capacity);
+/* Running totals over the series and the pixels held open (waits). */
+SF_API int sf_engine_group_counts(sf_engine *engine, sf_counts *out, uint64_t *live);
+/* The spots, and their pixels, finished by the last run (waits); -2 and *n
+ * set if `capacity` is too small. Spot::first counts from the series start. */
+SF_API int sf_engine_spots(sf_engine *engine, sf_spot *out, size_t capacity, size_t *n);
+SF_API int sf_engine_pixels(sf_engine *engine, sf_pixel *out, size_t capacity, size_t *n);
+/* Close everything still open (Labeller::finish); its spots are then the
+ * last run's. */
+SF_API int sf_engine_finish(sf_engine *engine);
 
 #ifdef __cplusplus
 }

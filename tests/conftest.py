@@ -28,6 +28,19 @@ def as_records(raw, dtype):
     return np.ascontiguousarray(raw).view(dtype).reshape(-1)
 
 
+def same_spots(got, want):
+    """Spot rows equal field by field, bit for bit. The 4 padding bytes of a
+    Spot carry no value (the reference leaves them indeterminate), so rows
+    are not compared as raw bytes."""
+    assert len(got) == len(want), (len(got), len(want))
+    for name in want.dtype.names:
+        a, b = np.ascontiguousarray(got[name]), np.ascontiguousarray(want[name])
+        if a.tobytes() != b.tobytes():
+            k = int(np.nonzero((a.view(np.uint8).reshape(len(a), -1) !=
+                                b.view(np.uint8).reshape(len(b), -1)).any(1))[0][0])
+            raise AssertionError(f"spot {k} field {name}: {got[k]} vs {want[k]}")
+
+
 @pytest.fixture(scope="session")
 def gpu_lib():
     import dials_metal_spotfinder_b200 as sf

@@ -89,3 +89,53 @@ def test_16m_batch_matches_oracle(gpu_lib):
         eng.synchronize()
         for f, img in enumerate(frames):
             assert eng.signal(0, f).tobytes() == O.dext(img)[1].tobytes()
+
+
+def run_series_through_engine(frames, batch, graph, slots=2, two_d=False):
+    """Every frame of a series through the engine with grouping, `batch`
+    frames per run; returns all spots, pixels and the final counts."""
+    from dials_metal_spotfinder_b200.engine import Engine
+    shape = frames[0].shape
+    spots, pixels = [], []
+    with Engine([shape] * batch, frames[0].dtype, slots=slots) as eng:
+        eng.enable_grouping(first_frame=0, two_d=two_d)
+        eng.use_graph(graph)
+        nb = len(frames) // batch
+        for b in range(nb):
+            slot = b % slots
+            for f in range(batch):
+                eng.upload(slot, f, frames[b * batch + f])
+            eng.run(slot)
+            spots.append(eng.spots())
+            pixels.append(eng.pixels())
+        eng.finish()
+        spots.append(eng.spots())
+        pixels.append(eng.pixels())
+        counts, live = eng.group_counts()
+    return np.concatenate(spots), np.concatenate(pixels), counts
+
+
+@pytest.mark.parametrize("batch,graph,two_d", [(1, False, False), (3, False, False),
+                                               (3, True, False), (2, True, True)])
+def test_engine_grouping_matches_oracle(gpu_lib, batch, graph, two_d):
+    from conftest import same_spots
+    from dials_metal_spotfinder_b200 import synth
+    series = synth.small()
+    frames = [series.frame(f) for f in range(12)]
+    spots, pixels, counts = run_series_through_engine(frames, batch, graph, two_d=two_d)
+    want = O.group([O.dext(img)[1] for img in frames], *frames[0].shape, two_d=two_d)
+    assert counts == want.counts
+    same_spots(spots, want.spots)
+    assert pixels.tobytes() == want.pixels.tobytes()
+
+
+def test_engine_grouping_4m(gpu_lib):
+    from conftest import same_spots
+    from dials_metal_spotfinder_b200 import synth
+    series = synth.eiger_4m(frames=8)
+    frames = [series.frame(f) for f in range(8)]
+    spots, pixels, counts = run_series_through_engine(frames, 4, True)
+    want = O.group([O.dext(img)[1] for img in frames], *frames[0].shape)
+    assert counts == want.counts
+    same_spots(spots, want.spots)
+    assert pixels.tobytes() == want.pixels.tobytes()
