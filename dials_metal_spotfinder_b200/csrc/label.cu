@@ -73,6 +73,9 @@ struct LabArgs {
   Pixel *kept;
   uint64_t *seg_start, *seg_count;
   int64_t *seg_z;
+  uint32_t *tab;       // block tables of the batch frames, nblk each
+  uint32_t *carry_tab; // block table of the carry's last frame
+  uint64_t nblk;
   LabelScalars *sc;
 };
 
@@ -114,19 +117,6 @@ __device__ __forceinline__ void uf_unite(uint32_t *parent, uint32_t a, uint32_t 
       return;
     a = old;
   }
-}
-
-// First position in [lo, hi) whose index is >= target.
-__device__ __forceinline__ uint64_t lower_bound(const uint32_t *ix, uint64_t lo, uint64_t hi,
-                                                uint32_t target) {
-  while (lo < hi) {
-    const uint64_t mid = (lo + hi) >> 1;
-    if (ix[mid] < target)
-      lo = mid + 1;
-    else
-      hi = mid;
-  }
-  return lo;
 }
 
 __device__ __forceinline__ int segment_of(const uint64_t *seg_start, int nseg, uint64_t g) {
@@ -211,6 +201,34 @@ __global__ void lab_setup(LabArgs a) {
   sc->accepted_pack = 0;
 }
 
+// Block tables. For a frame's list, entry b is the position (within the
+// list) of the first pixel whose index is at least 64 b, or kNone when there
+// is none; so the pixels of block b are the positions [tab[b], tab[b+1]).
+// A lookup of one index is then a scan of about two entries.
+constexpr int kBlockShift = 6;
+
+__device__ __forceinline__ const uint32_t *table_of(const LabArgs &a, int s, int first_batch_seg) {
+  return s < first_batch_seg ? a.carry_tab : a.tab + static_cast<uint64_t>(s - first_batch_seg) * a.nblk;
+}
+
+// Position of the pixel with index t in the list at [s0, s0 + count), or kNone.
+__device__ __forceinline__ uint64_t lookup(const LabArgs &a, const uint32_t *tab, uint64_t s0,
+                                           uint64_t count, uint32_t t) {
+  const uint64_t b = t >> kBlockShift;
+  uint32_t p0 = tab[b];
+  uint32_t p1 = b + 1 < a.nblk ? tab[b + 1] : kNone;
+  const uint64_t q0 = p0 == kNone ? count : p0;
+  const uint64_t q1 = p1 == kNone ? count : p1;
+  for (uint64_t p = q0; p < q1; p++) {
+    const uint32_t v = a.ix[s0 + p];
+    if (v == t)
+      return s0 + p;
+    if (v > t)
+      break;
+  }
+  return ~0ull;
+}
+
 __global__ void __launch_bounds__(kThreads) lab_gather(LabArgs a) {
   const LabelScalars *sc = a.sc;
   const uint64_t n = sc->n, carry = sc->carry_n;
@@ -224,11 +242,20 @@ __global__ void __launch_bounds__(kThreads) lab_gather(LabArgs a) {
     if (g >= carry) {
       const int s = segment_of(a.seg_start, nseg, g);
       const int f = s - first_batch_seg;
-      const SignalPixel px = a.lists[a.offs[f] + (g - a.seg_start[s])];
+      const uint64_t i = g - a.seg_start[s];
+      const SignalPixel *list = a.lists + a.offs[f];
+      const SignalPixel px = list[i];
       a.fr[g] = static_cast<int32_t>(a.seg_z[s]);
       a.ix[g] = px.index;
       a.val[g] = px.value;
       a.par[g] = static_cast<uint32_t>(g);
+      // This pixel is the first of every block from the one after the
+      // previous pixel's up to its own.
+      uint32_t *tab = a.tab + static_cast<uint64_t>(f) * a.nblk;
+      const uint64_t b1 = px.index >> kBlockShift;
+      const uint64_t b0 = i == 0 ? 0 : (list[i - 1].index >> kBlockShift) + 1;
+      for (uint64_t b = b0; b <= b1; b++)
+        tab[b] = static_cast<uint32_t>(i);
     }
   }
 }
@@ -237,6 +264,7 @@ __global__ void __launch_bounds__(kThreads) lab_link(LabArgs a) {
   const LabelScalars *sc = a.sc;
   const uint64_t n = sc->n, carry = sc->carry_n;
   const int nseg = static_cast<int>(sc->nseg);
+  const int first_batch_seg = carry > 0 ? 1 : 0;
   const uint32_t W = static_cast<uint32_t>(a.width);
   for (uint64_t g = carry + gtid(); g < n; g += gstride()) {
     const int s = segment_of(a.seg_start, nseg, g);
@@ -247,19 +275,29 @@ __global__ void __launch_bounds__(kThreads) lab_link(LabArgs a) {
       uf_unite(a.par, static_cast<uint32_t>(g), static_cast<uint32_t>(g - 1));
     // the pixel above (src/dials_spots.cc:115-123)
     if (idx >= W) {
-      const uint64_t j = lower_bound(a.ix, s0, g, idx - W);
-      if (j < g && a.ix[j] == idx - W)
+      const uint64_t j = lookup(a, table_of(a, s, first_batch_seg), s0, a.seg_count[s], idx - W);
+      if (j != ~0ull)
         uf_unite(a.par, static_cast<uint32_t>(g), static_cast<uint32_t>(j));
     }
     // the same pixel on the previous frame, if it is the frame before
     // (src/dials_spots.cc:128-137)
     if (!a.two_d && s > 0 && a.seg_z[s - 1] + 1 == a.seg_z[s]) {
-      const uint64_t p0 = a.seg_start[s - 1], p1 = p0 + a.seg_count[s - 1];
-      const uint64_t j = lower_bound(a.ix, p0, p1, idx);
-      if (j < p1 && a.ix[j] == idx)
+      const uint64_t j = lookup(a, table_of(a, s - 1, first_batch_seg), a.seg_start[s - 1],
+                                a.seg_count[s - 1], idx);
+      if (j != ~0ull)
         uf_unite(a.par, static_cast<uint32_t>(g), static_cast<uint32_t>(j));
     }
   }
+}
+
+// After the batch: the last frame's table becomes the carry's, since every
+// pixel of the last frame is carried, in the same order.
+__global__ void __launch_bounds__(kThreads) lab_keep_table(LabArgs a) {
+  if (a.nframes == 0 || a.close_all || a.two_d)
+    return;
+  const uint32_t *last = a.tab + static_cast<uint64_t>(a.nframes - 1) * a.nblk;
+  for (uint64_t b = gtid(); b < a.nblk; b += gstride())
+    a.carry_tab[b] = last[b];
 }
 
 __global__ void __launch_bounds__(kThreads) lab_flatten(LabArgs a) {
@@ -350,23 +388,46 @@ __device__ void sort_positions(uint32_t *v, uint32_t n) {
   }
 }
 
+// The member data a spot pass reads: from global memory through the member
+// positions, or from the per-warp copy in shared memory.
+struct GlobalMembers {
+  const LabArgs *a;
+  const uint32_t *m;
+  __device__ __forceinline__ void get(uint32_t k, uint32_t *idx, uint32_t *v, int32_t *z) const {
+    const uint32_t g = m[k];
+    *idx = a->ix[g];
+    *v = a->val[g];
+    *z = a->fr[g];
+  }
+};
+struct SharedMembers {
+  const uint32_t *ix, *val;
+  const int32_t *fr;
+  __device__ __forceinline__ void get(uint32_t k, uint32_t *idx, uint32_t *v, int32_t *z) const {
+    *idx = ix[k];
+    *v = val[k];
+    *z = fr[k];
+  }
+};
+
 // The per-component arithmetic of src/dials_spots.cc:221-360, in the
 // reference's order, one IEEE rounding per operation (explicit _rn so that
 // nothing is fused). Returns whether the spot passes the peak-centroid
 // filter; fills *spot either way.
-__device__ bool spot_pass(const LabArgs &a, const uint32_t *m, uint32_t n, Spot *spot) {
-  const uint32_t W = static_cast<uint32_t>(a.width);
+template <typename Members>
+__device__ bool spot_pass(uint32_t W, double max_sep, const Members &mem, uint32_t n,
+                          Spot *spot) {
   const double pixel_variance = 1.0 / 12.0;
   double sum = 0.0, sum_sq = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
   int32_t x0 = 0, x1 = 0, y0 = 0, y1 = 0, z0 = 0, z1 = 0;
   uint32_t peak_value = 0;
   double px = 0.0, py = 0.0, pz = 0.0;
   for (uint32_t k = 0; k < n; k++) {
-    const uint32_t g = m[k];
-    const uint32_t idx = a.ix[g];
+    uint32_t idx, v;
+    int32_t z;
+    mem.get(k, &idx, &v, &z);
     const int32_t x = static_cast<int32_t>(idx % W);
     const int32_t y = static_cast<int32_t>(idx / W);
-    const int32_t z = a.fr[g];
     if (k == 0) {
       x0 = x; x1 = x + 1; y0 = y; y1 = y + 1; z0 = z; z1 = z + 1;
     } else {
@@ -374,7 +435,6 @@ __device__ bool spot_pass(const LabArgs &a, const uint32_t *m, uint32_t n, Spot 
       y0 = min(y0, y); y1 = max(y1, y + 1);
       z0 = min(z0, z); z1 = max(z1, z + 1);
     }
-    const uint32_t v = a.val[g];
     const double value = __uint2double_rn(v);
     const double cx = __dadd_rn(__int2double_rn(x), 0.5);
     const double cy = __dadd_rn(__int2double_rn(y), 0.5);
@@ -400,12 +460,13 @@ __device__ bool spot_pass(const LabArgs &a, const uint32_t *m, uint32_t n, Spot 
     double mz = __ddiv_rn(wz, sum);
     double dx2 = 0.0, dy2 = 0.0, dz2 = 0.0;
     for (uint32_t k = 0; k < n; k++) {
-      const uint32_t g = m[k];
-      const uint32_t idx = a.ix[g];
-      const double value = __uint2double_rn(a.val[g]);
+      uint32_t idx, v;
+      int32_t z;
+      mem.get(k, &idx, &v, &z);
+      const double value = __uint2double_rn(v);
       const double dx = __dsub_rn(__dadd_rn(__uint2double_rn(idx % W), 0.5), mx);
       const double dy = __dsub_rn(__dadd_rn(__uint2double_rn(idx / W), 0.5), my);
-      const double dz = __dsub_rn(__dadd_rn(__int2double_rn(a.fr[g]), 0.5), mz);
+      const double dz = __dsub_rn(__dadd_rn(__int2double_rn(z), 0.5), mz);
       dx2 = __dadd_rn(dx2, __dmul_rn(__dmul_rn(value, dx), dx));
       dy2 = __dadd_rn(dy2, __dmul_rn(__dmul_rn(value, dy), dy));
       dz2 = __dadd_rn(dz2, __dmul_rn(__dmul_rn(value, dz), dz));
@@ -430,73 +491,183 @@ __device__ bool spot_pass(const LabArgs &a, const uint32_t *m, uint32_t n, Spot 
     spot->position[1] = __ddiv_rn(__int2double_rn(y1 + y0), 2.0);
     spot->position[2] = __ddiv_rn(__int2double_rn(z1 + z0), 2.0);
   }
-  if (a.max_sep > 0.0) {
+  if (max_sep > 0.0) {
     const double dx = __dsub_rn(px, spot->position[0]);
     const double dy = __dsub_rn(py, spot->position[1]);
     const double dz = __dsub_rn(pz, spot->position[2]);
     const double d = __dsqrt_rn(
         __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
-    if (d > a.max_sep)
+    if (d > max_sep)
       return false;
   }
   return true;
 }
 
-__global__ void __launch_bounds__(kThreads) lab_accept(LabArgs a) {
+// One warp per finished component. The members (positions in the live set)
+// are sorted in shared memory by a warp bitonic network -- position order is
+// (frame, index) order -- and their pixels gathered there; every lane then
+// runs the same sequential pass, so the doubles accumulate in the
+// reference's order and the result is warp-uniform. Components larger than
+// the per-warp buffer (possible only with max_spot_size above it) take a
+// slower path through global memory.
+constexpr int kCompWarps = 4;
+constexpr uint32_t kCompCap = 1024;
+
+struct WarpBuffers {
+  uint32_t *g, *ix, *val;
+  int32_t *fr;
+};
+
+__device__ __forceinline__ WarpBuffers warp_buffers(unsigned char *smem, int warp) {
+  WarpBuffers b;
+  uint32_t *base = reinterpret_cast<uint32_t *>(smem) + static_cast<size_t>(warp) * 4 * kCompCap;
+  b.g = base;
+  b.ix = base + kCompCap;
+  b.val = base + 2 * kCompCap;
+  b.fr = reinterpret_cast<int32_t *>(base + 3 * kCompCap);
+  return b;
+}
+
+__device__ void warp_sort(uint32_t *s, uint32_t n, int lane) {
+  uint32_t p = 2;
+  while (p < n)
+    p <<= 1;
+  for (uint32_t i = n + lane; i < p; i += 32)
+    s[i] = kNone;
+  __syncwarp();
+  for (uint32_t k = 2; k <= p; k <<= 1) {
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      for (uint32_t i = lane; i < p; i += 32) {
+        const uint32_t l = i ^ j;
+        if (l > i) {
+          const uint32_t x = s[i], y = s[l];
+          if ((x > y) == ((i & k) == 0)) {
+            s[i] = y;
+            s[l] = x;
+          }
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// Loads (sorting if asked) a component's members and their pixels into the
+// warp's buffers.
+__device__ void load_members(const LabArgs &a, uint32_t *m, uint32_t n, bool sort,
+                             const WarpBuffers &b, int lane) {
+  for (uint32_t k = lane; k < n; k += 32)
+    b.g[k] = m[k];
+  __syncwarp();
+  if (sort) {
+    warp_sort(b.g, n, lane);
+    for (uint32_t k = lane; k < n; k += 32)
+      m[k] = b.g[k];
+  }
+  for (uint32_t k = lane; k < n; k += 32) {
+    const uint32_t g = b.g[k];
+    b.ix[k] = a.ix[g];
+    b.val[k] = a.val[g];
+    b.fr[k] = a.fr[g];
+  }
+  __syncwarp();
+}
+
+__global__ void __launch_bounds__(kCompWarps * 32) lab_accept(LabArgs a) {
+  extern __shared__ __align__(16) unsigned char comp_smem[];
   LabelScalars *sc = a.sc;
   const uint64_t closed = sc->closed;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const WarpBuffers b = warp_buffers(comp_smem, warp);
+  const uint32_t W = static_cast<uint32_t>(a.width);
   uint32_t separated = 0;
-  for (uint64_t r = gtid(); r < closed; r += gstride()) {
+  const uint64_t gw = gtid() >> 5, nw = gstride() >> 5;
+  for (uint64_t r = gw; r < closed; r += nw) {
     const uint32_t n = a.msize[r];
     if (n == 0) {
-      a.pack[r] = 0;
+      if (lane == 0)
+        a.pack[r] = 0;
       continue;
     }
     uint32_t *m = a.members + a.moff[r];
-    sort_positions(m, n);
-    Spot spot{}; // zeroed, padding included, so rows compare byte for byte
-    const bool ok = spot_pass(a, m, n, &spot);
-    if (!ok) {
-      separated++;
-      a.msize[r] = 0;
-      a.pack[r] = 0;
+    Spot spot{};
+    bool ok;
+    if (n <= kCompCap) {
+      load_members(a, m, n, true, b, lane);
+      ok = spot_pass(W, a.max_sep, SharedMembers{b.ix, b.val, b.fr}, n, &spot);
     } else {
-      a.pack[r] = (static_cast<uint64_t>(n) << 32) | 1u;
+      if (lane == 0)
+        sort_positions(m, n);
+      __syncwarp();
+      __threadfence_block();
+      ok = spot_pass(W, a.max_sep, GlobalMembers{&a, m}, n, &spot);
     }
+    if (lane == 0) {
+      if (!ok) {
+        separated++;
+        a.msize[r] = 0;
+        a.pack[r] = 0;
+      } else {
+        a.pack[r] = (static_cast<uint64_t>(n) << 32) | 1u;
+      }
+    }
+    __syncwarp();
   }
-  if (separated)
+  if (lane == 0 && separated)
     atomicAdd(reinterpret_cast<unsigned long long *>(&sc->separated), separated);
 }
 
-__global__ void __launch_bounds__(kThreads) lab_write(LabArgs a) {
+__global__ void __launch_bounds__(kCompWarps * 32) lab_write(LabArgs a) {
+  extern __shared__ __align__(16) unsigned char comp_smem[];
   LabelScalars *sc = a.sc;
   const uint64_t closed = sc->closed;
   const uint64_t kept_base = sc->kept_total;
-  for (uint64_t r = gtid(); r < closed; r += gstride()) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const WarpBuffers b = warp_buffers(comp_smem, warp);
+  const uint32_t W = static_cast<uint32_t>(a.width);
+  const uint64_t gw = gtid() >> 5, nw = gstride() >> 5;
+  for (uint64_t r = gw; r < closed; r += nw) {
     const uint32_t n = a.msize[r];
     if (n == 0)
       continue;
     const uint64_t row = a.pack[r] & 0xffffffffu;
     const uint64_t pix = a.pack[r] >> 32;
-    const uint32_t *m = a.members + a.moff[r];
-    Spot spot{}; // zeroed, padding included, so rows compare byte for byte
-    spot_pass(a, m, n, &spot);
-    spot.first = kept_base + pix;
+    uint32_t *m = a.members + a.moff[r];
     if (row >= a.spot_cap || pix + n > a.live_cap) {
-      sc->status = kLabelSpotOverflow;
+      if (lane == 0)
+        sc->status = kLabelSpotOverflow;
       continue;
     }
-    a.spots[row] = spot;
-    for (uint32_t k = 0; k < n; k++) {
-      const uint32_t g = m[k];
-      Pixel p;
-      p.frame = a.fr[g];
-      p.index = a.ix[g];
-      p.value = a.val[g];
-      a.kept[pix + k] = p;
+    Spot spot{}; // zeroed, padding included, so rows compare byte for byte
+    if (n <= kCompCap) {
+      load_members(a, m, n, false, b, lane); // sorted by lab_accept
+      spot_pass(W, a.max_sep, SharedMembers{b.ix, b.val, b.fr}, n, &spot);
+      for (uint32_t k = lane; k < n; k += 32) {
+        Pixel p;
+        p.frame = b.fr[k];
+        p.index = b.ix[k];
+        p.value = b.val[k];
+        a.kept[pix + k] = p;
+      }
+    } else {
+      spot_pass(W, a.max_sep, GlobalMembers{&a, m}, n, &spot);
+      for (uint32_t k = lane; k < n; k += 32) {
+        const uint32_t g = m[k];
+        Pixel p;
+        p.frame = a.fr[g];
+        p.index = a.ix[g];
+        p.value = a.val[g];
+        a.kept[pix + k] = p;
+      }
     }
+    spot.first = kept_base + pix;
+    if (lane == 0)
+      a.spots[row] = spot;
+    __syncwarp();
   }
 }
+
+constexpr size_t kCompSmem = static_cast<size_t>(kCompWarps) * 4 * kCompCap * sizeof(uint32_t);
 
 __global__ void __launch_bounds__(kThreads) lab_open(LabArgs a) {
   const uint64_t n = a.sc->n;
@@ -557,6 +728,15 @@ DeviceLabeller::DeviceLabeller(int height, int width, const GroupOptions &option
     throw std::invalid_argument("dials_spots: frame too large");
   check(cudaMalloc(&sc_, sizeof(LabelScalars)), "cudaMalloc labeller scalars");
   check(cudaMemset(sc_, 0, sizeof(LabelScalars)), "clearing labeller scalars");
+  nblk_ = ((static_cast<uint64_t>(height) * width) >> kBlockShift) + 2;
+  check(cudaMalloc(&carry_tab_, nblk_ * sizeof(uint32_t)), "cudaMalloc carry table");
+  check(cudaFuncSetAttribute(lab_accept, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(kCompSmem)),
+        "cudaFuncSetAttribute");
+  check(cudaFuncSetAttribute(lab_write, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(kCompSmem)),
+        "cudaFuncSetAttribute");
+  grid_ = static_cast<unsigned>(device_sm_count() * 8);
   check(cudaMallocHost(&z_stage_, sizeof(int64_t)), "cudaMallocHost");
   check(cudaStreamSynchronize(cudaStreamLegacy), "clearing labeller scalars");
 }
@@ -564,6 +744,7 @@ DeviceLabeller::DeviceLabeller(int height, int width, const GroupOptions &option
 DeviceLabeller::~DeviceLabeller() {
   release();
   cudaFree(sc_);
+  cudaFree(carry_tab_);
   if (z_stage_)
     cudaFreeHost(z_stage_);
 }
@@ -578,9 +759,10 @@ void DeviceLabeller::release() {
   }
   void *ptrs[] = {root_, size_, rank_of_root_, cursor_, lastz_, bits_, bcnt_, comp_root_,
                   msize_, moff_, members_, pack_, open_, spots_out_, kept_out_, seg_start_,
-                  seg_count_, seg_z_};
+                  seg_count_, seg_z_, tab_};
   for (void *p : ptrs)
     cudaFree(p);
+  tab_ = nullptr;
   root_ = size_ = rank_of_root_ = cursor_ = nullptr;
   lastz_ = nullptr;
   bits_ = bcnt_ = comp_root_ = msize_ = moff_ = members_ = open_ = nullptr;
@@ -645,6 +827,7 @@ void DeviceLabeller::reserve(uint64_t batch_pixels, int max_frames, uint64_t car
     alloc(&seg_start_, fc + 1, "segments");
     alloc(&seg_count_, fc + 1, "segments");
     alloc(&seg_z_, fc + 1, "segments");
+    alloc(&tab_, static_cast<uint64_t>(fc) * nblk_, "block tables");
     scan32_.reserve((fc + 1) * nwmax);
     scan32_.reserve(live);
     scan64_.reserve(live);
@@ -724,13 +907,20 @@ void DeviceLabeller::enqueue(int nframes, const SignalPixel *lists, const uint64
   a.seg_start = seg_start_;
   a.seg_count = seg_count_;
   a.seg_z = seg_z_;
+  a.tab = tab_;
+  a.carry_tab = carry_tab_;
+  a.nblk = nblk_;
   a.sc = sc_;
 
-  const unsigned grid = static_cast<unsigned>(device_sm_count() * 8);
+  const unsigned grid = grid_;
   LabelScalars *sc = sc_;
+  if (nframes > 0)
+    check(cudaMemsetAsync(tab_, 0xff, static_cast<uint64_t>(nframes) * nblk_ * sizeof(uint32_t), s),
+          "clearing block tables");
   lab_setup<<<1, 32, 0, s>>>(a);
   lab_gather<<<grid, kThreads, 0, s>>>(a);
   lab_link<<<grid, kThreads, 0, s>>>(a);
+  lab_keep_table<<<grid, kThreads, 0, s>>>(a);
   lab_flatten<<<grid, kThreads, 0, s>>>(a);
   lab_mark<<<grid, kThreads, 0, s>>>(a);
   const uint64_t nwmax = live_cap_ / 32 + 1;
@@ -739,9 +929,9 @@ void DeviceLabeller::enqueue(int nframes, const SignalPixel *lists, const uint64
   lab_rank<<<grid, kThreads, 0, s>>>(a);
   scan32_.run(msize_, moff_, &sc->closed, 1, live_cap_, &sc->members32, s);
   lab_scatter<<<grid, kThreads, 0, s>>>(a);
-  lab_accept<<<grid, kThreads, 0, s>>>(a);
+  lab_accept<<<grid, kCompWarps * 32, kCompSmem, s>>>(a);
   scan64_.run(pack_, pack_, &sc->closed, 1, live_cap_, &sc->accepted_pack, s);
-  lab_write<<<grid, kThreads, 0, s>>>(a);
+  lab_write<<<grid, kCompWarps * 32, kCompSmem, s>>>(a);
   lab_open<<<grid, kThreads, 0, s>>>(a);
   scan32_.run(open_, open_, &sc->n, 1, live_cap_, &sc->open32, s);
   lab_carry<<<grid, kThreads, 0, s>>>(a);

@@ -134,6 +134,10 @@ private:
   uint64_t *seg_start_ = nullptr; // per batch segment: start, count (device)
   uint64_t *seg_count_ = nullptr;
   int64_t *seg_z_ = nullptr;
+  uint32_t *tab_ = nullptr;       // block tables of the batch frames
+  uint32_t *carry_tab_ = nullptr; // block table of the carry's last frame
+  uint64_t nblk_ = 0;
+  unsigned grid_ = 0;
   LabelScalars *sc_ = nullptr;
   int64_t *z_stage_ = nullptr; // pinned
 
