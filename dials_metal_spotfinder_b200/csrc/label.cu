@@ -66,7 +66,10 @@ struct LabArgs {
   int32_t *lastz;
   uint32_t *rank_of_root, *cursor;
   uint32_t *bits, *bcnt;
-  uint32_t *comp_root, *msize, *moff, *members;
+  uint32_t *comp_root, *msize, *members;
+  uint64_t *mpk;
+  Spot *spot_tmp;
+  Pixel *pix_tmp;
   uint64_t *pack;
   uint32_t *open;
   Spot *spots;
@@ -197,7 +200,8 @@ __global__ void lab_setup(LabArgs a) {
   sc->seg_len = static_cast<uint64_t>(nseg) * sc->nw;
   sc->signal_pixels += pos - carry;
   sc->next_carry_last_start = ~0ull;
-  sc->closed32 = sc->members32 = sc->open32 = 0;
+  sc->closed32 = sc->open32 = 0;
+  sc->members_pack = 0;
   sc->accepted_pack = 0;
 }
 
@@ -229,33 +233,55 @@ __device__ __forceinline__ uint64_t lookup(const LabArgs &a, const uint32_t *tab
   return ~0ull;
 }
 
+// The new pixels' lists are copied after the carried pixels; per-root
+// fields are cleared. Each new pixel's parent is set to the first pixel of
+// its horizontal run (left neighbours, src/dials_spots.cc:106-110) within its
+// 32-aligned chunk of positions, found with one ballot, so that the trees
+// start one level deep; a run that enters a chunk from the previous one is
+// joined by lab_link at the chunk's first position.
 __global__ void __launch_bounds__(kThreads) lab_gather(LabArgs a) {
   const LabelScalars *sc = a.sc;
   const uint64_t n = sc->n, carry = sc->carry_n;
   const int nseg = static_cast<int>(sc->nseg);
   const int first_batch_seg = carry > 0 ? 1 : 0;
-  for (uint64_t g = gtid(); g < n; g += gstride()) {
-    a.size[g] = 0;
-    a.lastz[g] = INT_MIN;
-    a.rank_of_root[g] = kNone;
-    a.cursor[g] = 0;
-    if (g >= carry) {
-      const int s = segment_of(a.seg_start, nseg, g);
-      const int f = s - first_batch_seg;
-      const uint64_t i = g - a.seg_start[s];
-      const SignalPixel *list = a.lists + a.offs[f];
-      const SignalPixel px = list[i];
-      a.fr[g] = static_cast<int32_t>(a.seg_z[s]);
-      a.ix[g] = px.index;
-      a.val[g] = px.value;
-      a.par[g] = static_cast<uint32_t>(g);
-      // This pixel is the first of every block from the one after the
-      // previous pixel's up to its own.
-      uint32_t *tab = a.tab + static_cast<uint64_t>(f) * a.nblk;
-      const uint64_t b1 = px.index >> kBlockShift;
-      const uint64_t b0 = i == 0 ? 0 : (list[i - 1].index >> kBlockShift) + 1;
-      for (uint64_t b = b0; b <= b1; b++)
-        tab[b] = static_cast<uint32_t>(i);
+  const uint32_t W = static_cast<uint32_t>(a.width);
+  const int lane = threadIdx.x & 31;
+  const uint64_t warps = gstride() >> 5;
+  for (uint64_t base = (gtid() >> 5) * 32; base < n; base += warps * 32) {
+    const uint64_t g = base + lane;
+    bool left = false;
+    if (g < n) {
+      a.size[g] = 0;
+      a.lastz[g] = INT_MIN;
+      a.rank_of_root[g] = kNone;
+      a.cursor[g] = 0;
+      if (g >= carry) {
+        const int s = segment_of(a.seg_start, nseg, g);
+        const int f = s - first_batch_seg;
+        const uint64_t i = g - a.seg_start[s];
+        const SignalPixel *list = a.lists + a.offs[f];
+        const SignalPixel px = list[i];
+        a.fr[g] = static_cast<int32_t>(a.seg_z[s]);
+        a.ix[g] = px.index;
+        a.val[g] = px.value;
+        const uint32_t prev = i == 0 ? 0u : list[i - 1].index;
+        left = i > 0 && px.index % W != 0 && prev + 1 == px.index;
+        // This pixel is the first of every block from the one after the
+        // previous pixel's up to its own.
+        uint32_t *tab = a.tab + static_cast<uint64_t>(f) * a.nblk;
+        const uint64_t b1 = px.index >> kBlockShift;
+        const uint64_t b0 = i == 0 ? 0 : (prev >> kBlockShift) + 1;
+        for (uint64_t b = b0; b <= b1; b++)
+          tab[b] = static_cast<uint32_t>(i);
+      }
+    }
+    const uint32_t linked = __ballot_sync(kFull, left);
+    if (g < n && g >= carry) {
+      // the run's first lane in this chunk: the highest lane at or below
+      // this one that is not joined to its left neighbour
+      const uint32_t starts = ~linked & (0xffffffffu >> (31 - lane));
+      const int first = starts ? 31 - __clz(starts) : 0;
+      a.par[g] = static_cast<uint32_t>(base + first);
     }
   }
 }
@@ -270,8 +296,9 @@ __global__ void __launch_bounds__(kThreads) lab_link(LabArgs a) {
     const int s = segment_of(a.seg_start, nseg, g);
     const uint64_t s0 = a.seg_start[s];
     const uint32_t idx = a.ix[g];
-    // the pixel to the left, in the same row (src/dials_spots.cc:106-110)
-    if (g > s0 && idx % W != 0 && a.ix[g - 1] + 1 == idx)
+    // the pixel to the left, where a run crosses into a new 32-position
+    // chunk (within a chunk lab_gather has already joined it)
+    if ((g & 31) == 0 && g > s0 && idx % W != 0 && a.ix[g - 1] + 1 == idx)
       uf_unite(a.par, static_cast<uint32_t>(g), static_cast<uint32_t>(g - 1));
     // the pixel above (src/dials_spots.cc:115-123)
     if (idx >= W) {
@@ -349,6 +376,7 @@ __global__ void __launch_bounds__(kThreads) lab_rank(LabArgs a) {
     const uint32_t size = a.size[g];
     const bool keep = size >= a.min_size && size <= a.max_size;
     a.msize[rank] = keep ? size : 0u;
+    a.mpk[rank] = keep ? (static_cast<uint64_t>(size) | (1ull << 32)) : 0ull;
     small += size < a.min_size;
     large += size > a.max_size;
   }
@@ -366,7 +394,7 @@ __global__ void __launch_bounds__(kThreads) lab_scatter(LabArgs a) {
     if (rank == kNone || a.msize[rank] == 0)
       continue;
     const uint32_t at = atomicAdd(&a.cursor[r], 1u);
-    a.members[a.moff[rank] + at] = static_cast<uint32_t>(g);
+    a.members[static_cast<uint32_t>(a.mpk[rank]) + at] = static_cast<uint32_t>(g);
   }
 }
 
@@ -573,6 +601,161 @@ __device__ void load_members(const LabArgs &a, uint32_t *m, uint32_t n, bool sor
   __syncwarp();
 }
 
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1)
+    v += __shfl_xor_sync(kFull, v, d);
+  return v;
+}
+__device__ __forceinline__ int32_t warp_min(int32_t v) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1)
+    v = min(v, __shfl_xor_sync(kFull, v, d));
+  return v;
+}
+__device__ __forceinline__ int32_t warp_max(int32_t v) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1)
+    v = max(v, __shfl_xor_sync(kFull, v, d));
+  return v;
+}
+
+// The spot pass with the warp's 32 lanes sharing the work, for members in
+// shared memory. The first pass (count, sums, weighted sums, bbox, peak) is
+// a parallel reduction; it is taken only when every partial sum it can form
+// is exact in double -- integers (and halves, for the weighted sums) below
+// 2^52 -- so its result is the reference's sequential one bit for bit. The
+// second pass's terms value * d * d are rounded, so they are formed in
+// parallel but added in member order, one after another, as the reference
+// adds them. Returns false (and leaves *spot alone) if the first pass is not
+// exact for this component; *ok is the peak-centroid filter's verdict.
+__device__ bool spot_pass_warp(uint32_t W, double max_sep, const WarpBuffers &b, uint32_t n,
+                               int lane, Spot *spot, bool *ok) {
+  double sum = 0.0, sum_sq = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
+  int32_t x0 = INT_MAX, x1 = INT_MIN, y0 = INT_MAX, y1 = INT_MIN, z0 = INT_MAX, z1 = INT_MIN;
+  uint32_t peak_v = 0, peak_k = kNone, max_v = 0;
+  uint32_t max_c = 0;
+  for (uint32_t k = lane; k < n; k += 32) {
+    const uint32_t idx = b.ix[k], v = b.val[k];
+    const int32_t z = b.fr[k];
+    const int32_t x = static_cast<int32_t>(idx % W), y = static_cast<int32_t>(idx / W);
+    const double value = __uint2double_rn(v);
+    sum = __dadd_rn(sum, value);
+    sum_sq = __dadd_rn(sum_sq, __dmul_rn(value, value));
+    wx = __dadd_rn(wx, __dmul_rn(value, __dadd_rn(__int2double_rn(x), 0.5)));
+    wy = __dadd_rn(wy, __dmul_rn(value, __dadd_rn(__int2double_rn(y), 0.5)));
+    wz = __dadd_rn(wz, __dmul_rn(value, __dadd_rn(__int2double_rn(z), 0.5)));
+    x0 = min(x0, x); x1 = max(x1, x + 1);
+    y0 = min(y0, y); y1 = max(y1, y + 1);
+    z0 = min(z0, z); z1 = max(z1, z + 1);
+    if (v > peak_v) { // k rises within a lane: the lane's first maximum
+      peak_v = v;
+      peak_k = k;
+    }
+    max_c = max(max_c, max(max(static_cast<uint32_t>(x), static_cast<uint32_t>(y)),
+                           static_cast<uint32_t>(z < 0 ? -z : z)));
+  }
+  max_v = peak_v;
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    max_v = max(max_v, __shfl_xor_sync(kFull, max_v, d));
+    max_c = max(max_c, __shfl_xor_sync(kFull, max_c, d));
+  }
+  // |every partial sum| <= n * max_v * max(max_v, 2 (max_c + 1)), in units
+  // of 0.5 for the weighted sums: exact below 2^52.
+  const double bound = static_cast<double>(n) * static_cast<double>(max_v) *
+                       fmax(static_cast<double>(max_v), 2.0 * (static_cast<double>(max_c) + 1.0));
+  if (!(bound < 4503599627370496.0)) // 2^52
+    return false;
+  sum = warp_sum(sum);
+  sum_sq = warp_sum(sum_sq);
+  wx = warp_sum(wx);
+  wy = warp_sum(wy);
+  wz = warp_sum(wz);
+  x0 = warp_min(x0); x1 = warp_max(x1);
+  y0 = warp_min(y0); y1 = warp_max(y1);
+  z0 = warp_min(z0); z1 = warp_max(z1);
+  // the first maximum over the whole component: the largest value, then
+  // the lowest member index among lanes that hold it
+  uint32_t pk = peak_v == max_v ? peak_k : kNone;
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1)
+    pk = min(pk, __shfl_xor_sync(kFull, pk, d));
+  double px = 0.0, py = 0.0, pz = 0.0;
+  if (max_v > 0 && pk != kNone) {
+    px = __dadd_rn(__uint2double_rn(b.ix[pk] % W), 0.5);
+    py = __dadd_rn(__uint2double_rn(b.ix[pk] / W), 0.5);
+    pz = __dadd_rn(__int2double_rn(b.fr[pk]), 0.5);
+  }
+
+  const double pixel_variance = 1.0 / 12.0;
+  spot->bbox[0] = x0; spot->bbox[1] = x1;
+  spot->bbox[2] = y0; spot->bbox[3] = y1;
+  spot->bbox[4] = z0; spot->bbox[5] = z1;
+  spot->intensity = sum;
+  spot->intensity_variance = sum;
+  spot->n_signal = n;
+  if (sum > 0.0) {
+    const double mx = __ddiv_rn(wx, sum), my = __ddiv_rn(wy, sum);
+    double mz = __ddiv_rn(wz, sum);
+    double dx2 = 0.0, dy2 = 0.0, dz2 = 0.0;
+    for (uint32_t c = 0; c < n; c += 32) {
+      const uint32_t k = c + lane;
+      double tx = 0.0, ty = 0.0, tz = 0.0;
+      if (k < n) {
+        const uint32_t idx = b.ix[k];
+        const double value = __uint2double_rn(b.val[k]);
+        const double dx = __dsub_rn(__dadd_rn(__uint2double_rn(idx % W), 0.5), mx);
+        const double dy = __dsub_rn(__dadd_rn(__uint2double_rn(idx / W), 0.5), my);
+        const double dz = __dsub_rn(__dadd_rn(__int2double_rn(b.fr[k]), 0.5), mz);
+        tx = __dmul_rn(__dmul_rn(value, dx), dx);
+        ty = __dmul_rn(__dmul_rn(value, dy), dy);
+        tz = __dmul_rn(__dmul_rn(value, dz), dz);
+      }
+      const uint32_t cnt = min(32u, n - c);
+      for (uint32_t j = 0; j < cnt; j++) {
+        dx2 = __dadd_rn(dx2, __shfl_sync(kFull, tx, j));
+        dy2 = __dadd_rn(dy2, __shfl_sync(kFull, ty, j));
+        dz2 = __dadd_rn(dz2, __shfl_sync(kFull, tz, j));
+      }
+    }
+    const double ss = __dmul_rn(sum, sum);
+    if (ss > sum_sq) {
+      const double den = __dsub_rn(ss, sum_sq);
+      spot->variance[0] = __dadd_rn(__ddiv_rn(__ddiv_rn(__dmul_rn(dx2, sum), den), sum), pixel_variance);
+      spot->variance[1] = __dadd_rn(__ddiv_rn(__ddiv_rn(__dmul_rn(dy2, sum), den), sum), pixel_variance);
+      spot->variance[2] = __dadd_rn(__ddiv_rn(__ddiv_rn(__dmul_rn(dz2, sum), den), sum), pixel_variance);
+    } else {
+      spot->variance[0] = spot->variance[1] = spot->variance[2] = pixel_variance;
+    }
+    if (z1 == z0 + 1)
+      mz = __dadd_rn(__int2double_rn(z0), 0.5);
+    spot->position[0] = mx;
+    spot->position[1] = my;
+    spot->position[2] = mz;
+  } else {
+    spot->variance[0] = spot->variance[1] = spot->variance[2] = 0.0;
+    spot->position[0] = __ddiv_rn(__int2double_rn(x1 + x0), 2.0);
+    spot->position[1] = __ddiv_rn(__int2double_rn(y1 + y0), 2.0);
+    spot->position[2] = __ddiv_rn(__int2double_rn(z1 + z0), 2.0);
+  }
+  *ok = true;
+  if (max_sep > 0.0) {
+    const double dx = __dsub_rn(px, spot->position[0]);
+    const double dy = __dsub_rn(py, spot->position[1]);
+    const double dz = __dsub_rn(pz, spot->position[2]);
+    const double d = __dsqrt_rn(
+        __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+    if (d > max_sep)
+      *ok = false;
+  }
+  return true;
+}
+
+// Per finished component that passes the size filters: sort its members,
+// run the spot pass, and park the spot and its pixel records by the
+// component's size-filtered index and member offset until lab_write knows
+// where the accepted ones go.
 __global__ void __launch_bounds__(kCompWarps * 32) lab_accept(LabArgs a) {
   extern __shared__ __align__(16) unsigned char comp_smem[];
   LabelScalars *sc = a.sc;
@@ -589,20 +772,42 @@ __global__ void __launch_bounds__(kCompWarps * 32) lab_accept(LabArgs a) {
         a.pack[r] = 0;
       continue;
     }
-    uint32_t *m = a.members + a.moff[r];
-    Spot spot{};
+    const uint32_t moff = static_cast<uint32_t>(a.mpk[r]);
+    const uint32_t sidx = static_cast<uint32_t>(a.mpk[r] >> 32);
+    uint32_t *m = a.members + moff;
+    Spot spot{}; // zeroed, padding included, so rows compare byte for byte
     bool ok;
     if (n <= kCompCap) {
       load_members(a, m, n, true, b, lane);
-      ok = spot_pass(W, a.max_sep, SharedMembers{b.ix, b.val, b.fr}, n, &spot);
+      if (!spot_pass_warp(W, a.max_sep, b, n, lane, &spot, &ok))
+        ok = spot_pass(W, a.max_sep, SharedMembers{b.ix, b.val, b.fr}, n, &spot);
+      for (uint32_t k = lane; k < n; k += 32) {
+        Pixel p;
+        p.frame = b.fr[k];
+        p.index = b.ix[k];
+        p.value = b.val[k];
+        a.pix_tmp[moff + k] = p;
+      }
     } else {
       if (lane == 0)
         sort_positions(m, n);
       __syncwarp();
       __threadfence_block();
       ok = spot_pass(W, a.max_sep, GlobalMembers{&a, m}, n, &spot);
+      for (uint32_t k = lane; k < n; k += 32) {
+        const uint32_t g = m[k];
+        Pixel p;
+        p.frame = a.fr[g];
+        p.index = a.ix[g];
+        p.value = a.val[g];
+        a.pix_tmp[moff + k] = p;
+      }
     }
     if (lane == 0) {
+      if (sidx < a.spot_cap)
+        a.spot_tmp[sidx] = spot;
+      else
+        sc->status = kLabelSpotOverflow;
       if (!ok) {
         separated++;
         a.msize[r] = 0;
@@ -617,14 +822,12 @@ __global__ void __launch_bounds__(kCompWarps * 32) lab_accept(LabArgs a) {
     atomicAdd(reinterpret_cast<unsigned long long *>(&sc->separated), separated);
 }
 
-__global__ void __launch_bounds__(kCompWarps * 32) lab_write(LabArgs a) {
-  extern __shared__ __align__(16) unsigned char comp_smem[];
+// The accepted spots to their rows and their pixels to the kept list.
+__global__ void __launch_bounds__(kThreads) lab_write(LabArgs a) {
   LabelScalars *sc = a.sc;
   const uint64_t closed = sc->closed;
   const uint64_t kept_base = sc->kept_total;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const WarpBuffers b = warp_buffers(comp_smem, warp);
-  const uint32_t W = static_cast<uint32_t>(a.width);
+  const int lane = threadIdx.x & 31;
   const uint64_t gw = gtid() >> 5, nw = gstride() >> 5;
   for (uint64_t r = gw; r < closed; r += nw) {
     const uint32_t n = a.msize[r];
@@ -632,38 +835,20 @@ __global__ void __launch_bounds__(kCompWarps * 32) lab_write(LabArgs a) {
       continue;
     const uint64_t row = a.pack[r] & 0xffffffffu;
     const uint64_t pix = a.pack[r] >> 32;
-    uint32_t *m = a.members + a.moff[r];
-    if (row >= a.spot_cap || pix + n > a.live_cap) {
+    const uint32_t moff = static_cast<uint32_t>(a.mpk[r]);
+    const uint32_t sidx = static_cast<uint32_t>(a.mpk[r] >> 32);
+    if (row >= a.spot_cap || sidx >= a.spot_cap || pix + n > a.live_cap) {
       if (lane == 0)
         sc->status = kLabelSpotOverflow;
       continue;
     }
-    Spot spot{}; // zeroed, padding included, so rows compare byte for byte
-    if (n <= kCompCap) {
-      load_members(a, m, n, false, b, lane); // sorted by lab_accept
-      spot_pass(W, a.max_sep, SharedMembers{b.ix, b.val, b.fr}, n, &spot);
-      for (uint32_t k = lane; k < n; k += 32) {
-        Pixel p;
-        p.frame = b.fr[k];
-        p.index = b.ix[k];
-        p.value = b.val[k];
-        a.kept[pix + k] = p;
-      }
-    } else {
-      spot_pass(W, a.max_sep, GlobalMembers{&a, m}, n, &spot);
-      for (uint32_t k = lane; k < n; k += 32) {
-        const uint32_t g = m[k];
-        Pixel p;
-        p.frame = a.fr[g];
-        p.index = a.ix[g];
-        p.value = a.val[g];
-        a.kept[pix + k] = p;
-      }
-    }
-    spot.first = kept_base + pix;
-    if (lane == 0)
+    if (lane == 0) {
+      Spot spot = a.spot_tmp[sidx];
+      spot.first = kept_base + pix;
       a.spots[row] = spot;
-    __syncwarp();
+    }
+    for (uint32_t k = lane; k < n; k += 32)
+      a.kept[pix + k] = a.pix_tmp[moff + k];
   }
 }
 
@@ -733,9 +918,6 @@ DeviceLabeller::DeviceLabeller(int height, int width, const GroupOptions &option
   check(cudaFuncSetAttribute(lab_accept, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(kCompSmem)),
         "cudaFuncSetAttribute");
-  check(cudaFuncSetAttribute(lab_write, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(kCompSmem)),
-        "cudaFuncSetAttribute");
   grid_ = static_cast<unsigned>(device_sm_count() * 8);
   check(cudaMallocHost(&z_stage_, sizeof(int64_t)), "cudaMallocHost");
   check(cudaStreamSynchronize(cudaStreamLegacy), "clearing labeller scalars");
@@ -758,15 +940,17 @@ void DeviceLabeller::release() {
     l = Live();
   }
   void *ptrs[] = {root_, size_, rank_of_root_, cursor_, lastz_, bits_, bcnt_, comp_root_,
-                  msize_, moff_, members_, pack_, open_, spots_out_, kept_out_, seg_start_,
+                  msize_, mpk_, spot_tmp_, pix_tmp_, members_, pack_, open_, spots_out_, kept_out_, seg_start_,
                   seg_count_, seg_z_, tab_};
   for (void *p : ptrs)
     cudaFree(p);
   tab_ = nullptr;
   root_ = size_ = rank_of_root_ = cursor_ = nullptr;
   lastz_ = nullptr;
-  bits_ = bcnt_ = comp_root_ = msize_ = moff_ = members_ = open_ = nullptr;
-  pack_ = nullptr;
+  bits_ = bcnt_ = comp_root_ = msize_ = members_ = open_ = nullptr;
+  mpk_ = pack_ = nullptr;
+  spot_tmp_ = nullptr;
+  pix_tmp_ = nullptr;
   spots_out_ = nullptr;
   kept_out_ = nullptr;
   seg_start_ = seg_count_ = nullptr;
@@ -818,11 +1002,13 @@ void DeviceLabeller::reserve(uint64_t batch_pixels, int max_frames, uint64_t car
     alloc(&bcnt_, (fc + 1) * nwmax, "bucket counts");
     alloc(&comp_root_, live, "components");
     alloc(&msize_, live, "member sizes");
-    alloc(&moff_, live, "member offsets");
+    alloc(&mpk_, live, "member offsets");
     alloc(&members_, live, "members");
     alloc(&pack_, live, "spot offsets");
     alloc(&open_, live, "open flags");
     alloc(&spots_out_, spot_cap, "spots");
+    alloc(&spot_tmp_, spot_cap, "spot scratch");
+    alloc(&pix_tmp_, live, "spot pixel scratch");
     alloc(&kept_out_, live, "spot pixels");
     alloc(&seg_start_, fc + 1, "segments");
     alloc(&seg_count_, fc + 1, "segments");
@@ -898,7 +1084,9 @@ void DeviceLabeller::enqueue(int nframes, const SignalPixel *lists, const uint64
   a.bcnt = bcnt_;
   a.comp_root = comp_root_;
   a.msize = msize_;
-  a.moff = moff_;
+  a.mpk = mpk_;
+  a.spot_tmp = spot_tmp_;
+  a.pix_tmp = pix_tmp_;
   a.members = members_;
   a.pack = pack_;
   a.open = open_;
@@ -927,11 +1115,11 @@ void DeviceLabeller::enqueue(int nframes, const SignalPixel *lists, const uint64
   scan32_.run(bcnt_, bcnt_, &sc->seg_len, 1, static_cast<uint64_t>(frame_cap_ + 1) * nwmax,
               &sc->closed32, s);
   lab_rank<<<grid, kThreads, 0, s>>>(a);
-  scan32_.run(msize_, moff_, &sc->closed, 1, live_cap_, &sc->members32, s);
+  scan64_.run(mpk_, mpk_, &sc->closed, 1, live_cap_, &sc->members_pack, s);
   lab_scatter<<<grid, kThreads, 0, s>>>(a);
   lab_accept<<<grid, kCompWarps * 32, kCompSmem, s>>>(a);
   scan64_.run(pack_, pack_, &sc->closed, 1, live_cap_, &sc->accepted_pack, s);
-  lab_write<<<grid, kCompWarps * 32, kCompSmem, s>>>(a);
+  lab_write<<<grid, kThreads, 0, s>>>(a);
   lab_open<<<grid, kThreads, 0, s>>>(a);
   scan32_.run(open_, open_, &sc->n, 1, live_cap_, &sc->open32, s);
   lab_carry<<<grid, kThreads, 0, s>>>(a);
