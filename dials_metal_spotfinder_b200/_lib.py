@@ -74,6 +74,7 @@ SIGNATURES = {
     "sf_set_device": (_I, [_I]),
     "sf_find_u16": (_I, [_P, _S, _S, _P, _S, ctypes.POINTER(_S)]),
     "sf_find_u32": (_I, [_P, _S, _S, _P, _S, ctypes.POINTER(_S)]),
+    "sf_find_u16_noalloc": (_I, [_P, _S, _S, _P, _S, ctypes.POINTER(_S), _P]),
     "sf_profile_stages": (None, [_I]),
     "sf_profile_stages_enabled": (_I, []),
     "sf_last_stage_times": (None, [_P]),

@@ -113,6 +113,26 @@ SF_API int sf_find_u16(const uint16_t *image, size_t height, size_t width, sf_si
 SF_API int sf_find_u32(const uint32_t *image, size_t height, size_t width, sf_signal_pixel *out,
                 size_t capacity, size_t *found);
 
+/* sf_find_u16 for callers that may not allocate device memory. No
+ * counterpart in the reference, whose gpu::find allocates per call.
+ *
+ * For plugins loaded into a host that owns the GPU's memory (a framework
+ * whose pool or caching allocator holds it) and for real-time loops where
+ * cudaMalloc / cudaFree would stall -- cudaFree synchronises the device.
+ * Same arguments, results and status codes as sf_find_u16, plus the stream
+ * to run on (NULL: the legacy default stream); it returns when the results
+ * are in `out`. It allocates nothing: it works in one 64 MiB device array
+ * that is part of the library (every GPU that loads the library holds it
+ * until exit) and returns -1, with the reason in sf_last_error(), for a
+ * frame whose buffers do not fit there (every frame of up to 6.2 million
+ * pixels at a width of at least 1024 fits on a 148-SM B200). The first call
+ * on each device looks the array's address up; make it before any stream
+ * capture. All calls share the array, so calls whose device work overlapped
+ * would race: each call holds a process-wide lock until its work is done. */
+SF_API int sf_find_u16_noalloc(const uint16_t *image, size_t height, size_t width,
+                               sf_signal_pixel *out, size_t capacity, size_t *found,
+                               void *stream);
+
 /* ---- stage profiling: src/dext_gpu.hh:79-116 ---------------------------- *
  * When on, sf_find_* records, for the calling thread, milliseconds spent in:
  * [0] upload (host to device), [1] the fused threshold kernel, [2] 0 (the
