@@ -289,11 +289,12 @@ __global__ void __launch_bounds__(kThreads) lab_gather(LabArgs a) {
 __global__ void __launch_bounds__(kThreads) lab_link(LabArgs a) {
   const LabelScalars *sc = a.sc;
   const uint64_t n = sc->n, carry = sc->carry_n;
-  const int nseg = static_cast<int>(sc->nseg);
   const int first_batch_seg = carry > 0 ? 1 : 0;
   const uint32_t W = static_cast<uint32_t>(a.width);
+  const int64_t z0 = sc->batch_z0;
   for (uint64_t g = carry + gtid(); g < n; g += gstride()) {
-    const int s = segment_of(a.seg_start, nseg, g);
+    // the batch's frames are consecutive: a new pixel's frame is its segment
+    const int s = first_batch_seg + static_cast<int>(a.fr[g] - z0);
     const uint64_t s0 = a.seg_start[s];
     const uint32_t idx = a.ix[g];
     // the pixel to the left, where a run crosses into a new 32-position
@@ -386,14 +387,33 @@ __global__ void __launch_bounds__(kThreads) lab_rank(LabArgs a) {
     atomicAdd(reinterpret_cast<unsigned long long *>(&sc->too_large), large);
 }
 
+// Member lists. A warp takes 32 consecutive positions; the lanes of one
+// component claim their slots with one atomic and fill them in lane order.
+// So each component's list is a set of runs, one per 32-position chunk it
+// has pixels in, each run ascending and within its chunk; lab_accept orders
+// the runs rather than the members.
 __global__ void __launch_bounds__(kThreads) lab_scatter(LabArgs a) {
   const uint64_t n = a.sc->n;
-  for (uint64_t g = gtid(); g < n; g += gstride()) {
-    const uint32_t r = a.root[g];
-    const uint32_t rank = a.rank_of_root[r];
-    if (rank == kNone || a.msize[rank] == 0)
+  const int lane = threadIdx.x & 31;
+  const uint64_t warps = gstride() >> 5;
+  for (uint64_t base = (gtid() >> 5) * 32; base < n; base += warps * 32) {
+    const uint64_t g = base + lane;
+    uint32_t r = kNone, rank = kNone;
+    if (g < n) {
+      r = a.root[g];
+      rank = a.rank_of_root[r];
+      if (rank != kNone && a.msize[rank] == 0)
+        rank = kNone;
+    }
+    const uint32_t key = rank == kNone ? kNone : r;
+    const uint32_t peers = __match_any_sync(kFull, key);
+    if (key == kNone)
       continue;
-    const uint32_t at = atomicAdd(&a.cursor[r], 1u);
+    const int leader = __ffs(peers) - 1;
+    uint32_t at = 0;
+    if (lane == leader)
+      at = atomicAdd(&a.cursor[r], static_cast<uint32_t>(__popc(peers)));
+    at = __shfl_sync(peers, at, leader) + __popc(peers & ((1u << lane) - 1u));
     a.members[static_cast<uint32_t>(a.mpk[rank]) + at] = static_cast<uint32_t>(g);
   }
 }
@@ -580,18 +600,101 @@ __device__ void warp_sort(uint32_t *s, uint32_t n, int lane) {
   }
 }
 
-// Loads (sorting if asked) a component's members and their pixels into the
+// Member k of b.g starts a run: the first member, or a different 32-position
+// chunk from the member before it.
+__device__ __forceinline__ bool run_start(const uint32_t *g, uint32_t k, uint32_t n) {
+  return k < n && (k == 0 || (g[k] >> 5) != (g[k - 1] >> 5));
+}
+
+// Puts the member positions in b.g (n <= kCompCap, as lab_scatter left them:
+// runs, one per chunk, each ascending) into ascending order by ordering the
+// runs: their chunks are sorted (the chunks of one component are distinct),
+// each run finds its rank by binary search, and every member moves once.
+// Uses b.ix, b.val and b.fr as scratch.
+__device__ void order_members(const WarpBuffers &b, uint32_t n, int lane) {
+  const uint32_t lt = (1u << lane) - 1u;
+  uint32_t runs = 0;
+  for (uint32_t c = 0; c < n; c += 32) {
+    const uint32_t k = c + lane;
+    const bool st = run_start(b.g, k, n);
+    const uint32_t flags = __ballot_sync(kFull, st);
+    if (st)
+      b.ix[runs + __popc(flags & lt)] = k; // where run j starts
+    runs += __popc(flags);
+  }
+  __syncwarp();
+  if (runs == 1)
+    return; // one chunk: already ascending
+  for (uint32_t j = lane; j < runs; j += 32)
+    b.val[j] = b.g[b.ix[j]] >> 5;
+  __syncwarp();
+  warp_sort(b.val, runs, lane); // the chunks, ascending
+  auto rank_of = [&](uint32_t key) {
+    uint32_t lo = 0, hi = runs;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (b.val[mid] < key)
+        lo = mid + 1;
+      else
+        hi = mid;
+    }
+    return lo;
+  };
+  for (uint32_t j = lane; j < runs; j += 32) {
+    const uint32_t s0 = b.ix[j];
+    const uint32_t s1 = j + 1 < runs ? b.ix[j + 1] : n;
+    b.fr[rank_of(b.g[s0] >> 5)] = static_cast<int32_t>(s1 - s0); // lengths in chunk order
+  }
+  __syncwarp();
+  uint32_t carry = 0; // exclusive scan of the lengths: each run's place
+  for (uint32_t c = 0; c < runs; c += 32) {
+    const uint32_t q = c + lane;
+    const uint32_t len = q < runs ? static_cast<uint32_t>(b.fr[q]) : 0u;
+    uint32_t inc = len;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t v = __shfl_up_sync(kFull, inc, d);
+      if (lane >= d)
+        inc += v;
+    }
+    if (q < runs)
+      b.fr[q] = static_cast<int32_t>(carry + inc - len);
+    carry += __shfl_sync(kFull, inc, 31);
+  }
+  __syncwarp();
+  for (uint32_t j = lane; j < runs; j += 32) {
+    const uint32_t s0 = b.ix[j];
+    const uint32_t off = static_cast<uint32_t>(b.fr[rank_of(b.g[s0] >> 5)]);
+    b.ix[j] = s0 | (off << 16); // start and place, both below kCompCap
+  }
+  __syncwarp();
+  uint32_t base = 0;
+  for (uint32_t c = 0; c < n; c += 32) {
+    const uint32_t k = c + lane;
+    const uint32_t flags = __ballot_sync(kFull, run_start(b.g, k, n));
+    // the run this member belongs to: the last start at or before it
+    const uint32_t r = base + __popc(flags & (lt | (1u << lane))) - 1;
+    if (k < n) {
+      const uint32_t packed = b.ix[r];
+      b.fr[(packed >> 16) + (k - (packed & 0xffffu))] = static_cast<int32_t>(b.g[k]);
+    }
+    base += __popc(flags);
+  }
+  __syncwarp();
+  for (uint32_t k = lane; k < n; k += 32)
+    b.g[k] = static_cast<uint32_t>(b.fr[k]);
+  __syncwarp();
+}
+
+// Loads (ordering if asked) a component's members and their pixels into the
 // warp's buffers.
 __device__ void load_members(const LabArgs &a, uint32_t *m, uint32_t n, bool sort,
                              const WarpBuffers &b, int lane) {
   for (uint32_t k = lane; k < n; k += 32)
     b.g[k] = m[k];
   __syncwarp();
-  if (sort) {
-    warp_sort(b.g, n, lane);
-    for (uint32_t k = lane; k < n; k += 32)
-      m[k] = b.g[k];
-  }
+  if (sort)
+    order_members(b, n, lane);
   for (uint32_t k = lane; k < n; k += 32) {
     const uint32_t g = b.g[k];
     b.ix[k] = a.ix[g];
