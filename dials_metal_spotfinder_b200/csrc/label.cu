@@ -199,7 +199,6 @@ __global__ void lab_setup(LabArgs a) {
   sc->nseg = nseg;
   sc->seg_len = static_cast<uint64_t>(nseg) * sc->nw;
   sc->signal_pixels += pos - carry;
-  sc->next_carry_last_start = ~0ull;
   sc->closed32 = sc->open32 = 0;
   sc->members_pack = 0;
   sc->accepted_pack = 0;
@@ -213,24 +212,6 @@ constexpr int kBlockShift = 6;
 
 __device__ __forceinline__ const uint32_t *table_of(const LabArgs &a, int s, int first_batch_seg) {
   return s < first_batch_seg ? a.carry_tab : a.tab + static_cast<uint64_t>(s - first_batch_seg) * a.nblk;
-}
-
-// Position of the pixel with index t in the list at [s0, s0 + count), or kNone.
-__device__ __forceinline__ uint64_t lookup(const LabArgs &a, const uint32_t *tab, uint64_t s0,
-                                           uint64_t count, uint32_t t) {
-  const uint64_t b = t >> kBlockShift;
-  uint32_t p0 = tab[b];
-  uint32_t p1 = b + 1 < a.nblk ? tab[b + 1] : kNone;
-  const uint64_t q0 = p0 == kNone ? count : p0;
-  const uint64_t q1 = p1 == kNone ? count : p1;
-  for (uint64_t p = q0; p < q1; p++) {
-    const uint32_t v = a.ix[s0 + p];
-    if (v == t)
-      return s0 + p;
-    if (v > t)
-      break;
-  }
-  return ~0ull;
 }
 
 // The new pixels' lists are copied after the carried pixels; per-root
@@ -286,6 +267,42 @@ __global__ void __launch_bounds__(kThreads) lab_gather(LabArgs a) {
   }
 }
 
+// First position (relative to the list at s0) whose index is at least t,
+// or count.
+__device__ __forceinline__ uint64_t first_at_least(const LabArgs &a, const uint32_t *tab,
+                                                   uint64_t s0, uint64_t count, uint32_t t) {
+  const uint32_t p = tab[t >> kBlockShift];
+  uint64_t q = p == kNone ? count : p;
+  while (q < count && a.ix[s0 + q] < t)
+    q++;
+  return q;
+}
+
+// Unites the run whose first pixel is g with every run of the list at s0
+// that has a pixel with an index in [lo, hi] (one row's span).
+__device__ __forceinline__ void unite_overlaps(const LabArgs &a, uint32_t g, const uint32_t *tab,
+                                               uint64_t s0, uint64_t count, uint32_t lo,
+                                               uint32_t hi) {
+  uint32_t prev = 0;
+  bool first = true;
+  for (uint64_t q = first_at_least(a, tab, s0, count, lo); q < count; q++) {
+    const uint32_t v = a.ix[s0 + q];
+    if (v > hi)
+      break;
+    if (first || v != prev + 1) // the first pixel of a run within the span
+      uf_unite(a.par, g, static_cast<uint32_t>(s0 + q));
+    first = false;
+    prev = v;
+  }
+}
+
+// The links of src/dials_spots.cc:106-137 -- left, up, and the same pixel on
+// the frame before -- taken a run at a time. A pixel joined to its left
+// neighbour already shares a tree with its run's first pixel (lab_gather),
+// except where the run crosses into a new 32-position chunk, which is joined
+// here. The first pixel of each run then unites it with every run of the row
+// above, and of the previous frame's same row, that overlaps its span: each
+// up or previous-frame edge of the run's pixels ends in one of those runs.
 __global__ void __launch_bounds__(kThreads) lab_link(LabArgs a) {
   const LabelScalars *sc = a.sc;
   const uint64_t n = sc->n, carry = sc->carry_n;
@@ -296,25 +313,26 @@ __global__ void __launch_bounds__(kThreads) lab_link(LabArgs a) {
     // the batch's frames are consecutive: a new pixel's frame is its segment
     const int s = first_batch_seg + static_cast<int>(a.fr[g] - z0);
     const uint64_t s0 = a.seg_start[s];
+    const uint64_t end = s0 + a.seg_count[s];
     const uint32_t idx = a.ix[g];
-    // the pixel to the left, where a run crosses into a new 32-position
-    // chunk (within a chunk lab_gather has already joined it)
-    if ((g & 31) == 0 && g > s0 && idx % W != 0 && a.ix[g - 1] + 1 == idx)
-      uf_unite(a.par, static_cast<uint32_t>(g), static_cast<uint32_t>(g - 1));
-    // the pixel above (src/dials_spots.cc:115-123)
-    if (idx >= W) {
-      const uint64_t j = lookup(a, table_of(a, s, first_batch_seg), s0, a.seg_count[s], idx - W);
-      if (j != ~0ull)
-        uf_unite(a.par, static_cast<uint32_t>(g), static_cast<uint32_t>(j));
+    if (g > s0 && idx % W != 0 && a.ix[g - 1] + 1 == idx) {
+      if ((g & 31) == 0)
+        uf_unite(a.par, static_cast<uint32_t>(g), static_cast<uint32_t>(g - 1));
+      continue;
     }
-    // the same pixel on the previous frame, if it is the frame before
-    // (src/dials_spots.cc:128-137)
-    if (!a.two_d && s > 0 && a.seg_z[s - 1] + 1 == a.seg_z[s]) {
-      const uint64_t j = lookup(a, table_of(a, s - 1, first_batch_seg), a.seg_start[s - 1],
-                                a.seg_count[s - 1], idx);
-      if (j != ~0ull)
-        uf_unite(a.par, static_cast<uint32_t>(g), static_cast<uint32_t>(j));
+    uint32_t last = idx; // the run's last index
+    for (uint64_t e = g + 1; e < end; e++) {
+      const uint32_t v = a.ix[e];
+      if (v != last + 1 || v % W == 0)
+        break;
+      last = v;
     }
+    if (idx >= W)
+      unite_overlaps(a, static_cast<uint32_t>(g), table_of(a, s, first_batch_seg), s0, end - s0,
+                     idx - W, last - W);
+    if (!a.two_d && s > 0 && a.seg_z[s - 1] + 1 == a.seg_z[s])
+      unite_overlaps(a, static_cast<uint32_t>(g), table_of(a, s - 1, first_batch_seg),
+                     a.seg_start[s - 1], a.seg_count[s - 1], idx, last);
   }
 }
 
@@ -328,13 +346,29 @@ __global__ void __launch_bounds__(kThreads) lab_keep_table(LabArgs a) {
     a.carry_tab[b] = last[b];
 }
 
+// Roots, component sizes and last frames. Lanes of one warp that share a
+// root (neighbours in a run, mostly) make one update between them.
 __global__ void __launch_bounds__(kThreads) lab_flatten(LabArgs a) {
   const uint64_t n = a.sc->n;
-  for (uint64_t g = gtid(); g < n; g += gstride()) {
-    const uint32_t r = uf_find(a.par, static_cast<uint32_t>(g));
-    a.root[g] = r;
-    atomicAdd(&a.size[r], 1u);
-    atomicMax(&a.lastz[r], a.fr[g]);
+  const int lane = threadIdx.x & 31;
+  const uint64_t warps = gstride() >> 5;
+  for (uint64_t base = (gtid() >> 5) * 32; base < n; base += warps * 32) {
+    const uint64_t g = base + lane;
+    uint32_t r = kNone;
+    int32_t z = INT_MIN;
+    if (g < n) {
+      r = uf_find(a.par, static_cast<uint32_t>(g));
+      a.root[g] = r;
+      z = a.fr[g];
+    }
+    const uint32_t peers = __match_any_sync(kFull, r);
+    int32_t zmax = z;
+    for (uint32_t m = peers & (peers - 1); m; m &= m - 1) // other lanes of the group
+      zmax = max(zmax, __shfl_sync(peers, z, __ffs(m) - 1));
+    if (r != kNone && lane == __ffs(peers) - 1) {
+      atomicAdd(&a.size[r], static_cast<uint32_t>(__popc(peers)));
+      atomicMax(&a.lastz[r], zmax);
+    }
   }
 }
 
@@ -966,7 +1000,6 @@ __global__ void __launch_bounds__(kThreads) lab_open(LabArgs a) {
 __global__ void __launch_bounds__(kThreads) lab_carry(LabArgs a) {
   LabelScalars *sc = a.sc;
   const uint64_t n = sc->n;
-  const int64_t zlast = last_batch_frame(a);
   for (uint64_t g = gtid(); g < n; g += gstride()) {
     const uint32_t r = a.root[g];
     if (a.rank_of_root[r] != kNone)
@@ -976,9 +1009,6 @@ __global__ void __launch_bounds__(kThreads) lab_carry(LabArgs a) {
     a.nix[at] = a.ix[g];
     a.nval[at] = a.val[g];
     a.npar[at] = a.open[r]; // the root is open too, and comes first
-    if (static_cast<int64_t>(a.fr[g]) == zlast)
-      atomicMin(reinterpret_cast<unsigned long long *>(&sc->next_carry_last_start),
-                static_cast<unsigned long long>(at));
   }
 }
 
@@ -996,7 +1026,10 @@ __global__ void lab_finalize(LabArgs a) {
   sc->batch_pixels = pixels;
   sc->carry_n = all ? 0 : sc->open32;
   sc->carry_last_z = last_batch_frame(a);
-  sc->carry_last_start = sc->carry_n > 0 ? sc->next_carry_last_start : 0;
+  // Every pixel of the last frame stays open (its components can still
+  // grow), so the carry's last frame starts where that frame's first pixel
+  // lands: its exclusive-scan value.
+  sc->carry_last_start = sc->carry_n > 0 ? a.open[a.seg_start[sc->nseg - 1]] : 0;
   sc->batch_z0 += a.nframes;
 }
 

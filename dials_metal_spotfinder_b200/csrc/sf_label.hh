@@ -57,7 +57,6 @@ struct LabelScalars {
   uint64_t carry_n;
   uint64_t carry_last_start; // first carried pixel on the carry's last frame
   int64_t carry_last_z;
-  uint64_t next_carry_last_start; // being found for the next batch
   // running totals over the series (src/dials_spots.hh:99-106)
   uint64_t signal_pixels, groups, too_small, too_large, separated, accepted;
   uint64_t kept_total; // pixels of accepted spots so far (Spot::first base)
