@@ -88,6 +88,7 @@ SIGNATURES = {
     "sf_labeller_live": (_S, [_P]),
     "sf_labeller_spots": (_I, [_P, _P, _S]),
     "sf_labeller_pixels": (_I, [_P, _P, _S]),
+    "sf_refl_write": (_I, [ctypes.c_char_p, _P, _S, _P, _S, _S, _P]),
     "sf_engine_create": (_I, [_I, _I, _P, _P, _P, ctypes.POINTER(_P)]),
     "sf_engine_destroy": (None, [_P]),
     "sf_engine_info": (_I, [_P, _P]),
@@ -108,6 +109,11 @@ SIGNATURES = {
     "sf_engine_pixels": (_I, [_P, _P, _S, ctypes.POINTER(_S)]),
     "sf_engine_finish": (_I, [_P]),
 }
+
+
+class ReflOptions(ctypes.Structure):
+    _fields_ = [("panel", ctypes.c_uint64), ("id", ctypes.c_int32), ("shoeboxes", ctypes.c_int32),
+                ("identifier", ctypes.c_char_p)]
 
 
 class EngineConfig(ctypes.Structure):

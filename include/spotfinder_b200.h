@@ -172,6 +172,28 @@ SF_API size_t sf_labeller_live(sf_labeller *labeller);
 SF_API int sf_labeller_spots(sf_labeller *labeller, sf_spot *out, size_t capacity);
 SF_API int sf_labeller_pixels(sf_labeller *labeller, sf_pixel *out, size_t capacity);
 
+/* ---- the reflection table: src/refl.hh:72-74 (refl::write) ------------- *
+ *
+ * Writes `spots` (with their pixels, `width` the frame width the labeller
+ * was given) to `path` as a DIALS .refl file, byte-identical to the
+ * reference's refl::write: the msgpack reflection table with bbox, flags
+ * (Strong), id, intensity.sum.value / .variance, n_signal, panel, the
+ * optional shoebox column (src/refl.cc:295-334, built on the device) and
+ * xyzobs.px.value / .variance. Returns -1 for a null argument or width 0,
+ * -4 for a spot whose pixels run past the list or lie outside its box or a
+ * column past msgpack's 4 GB limit, -3 when the file cannot be written or
+ * the device fails. */
+typedef struct sf_refl_options {
+  uint64_t panel;         /* one panel: 0 */
+  int32_t id;             /* the experiment every row belongs to */
+  int32_t shoeboxes;      /* write the shoebox column */
+  const char *identifier; /* the experiment identifier; NULL or "" for none */
+} sf_refl_options;
+
+SF_API int sf_refl_write(const char *path, const sf_spot *spots, size_t nspots,
+                         const sf_pixel *pixels, size_t npixels, size_t width,
+                         const sf_refl_options *options);
+
 /* ---- the batched engine ------------------------------------------------- *
  * No single reference counterpart: it replaces the reference's pattern of
  * -j host threads each calling gpu::find on one frame (src/find_spots.cc:

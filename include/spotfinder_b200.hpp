@@ -114,6 +114,30 @@ private:
   mutable CountsT counts_{};
 };
 
+// refl::write (src/refl.hh:72-74) over sf_refl_write: the same file, byte
+// for byte, with the shoebox column built on the device. Options: anything
+// with panel, id, identifier (std::string) and shoeboxes members
+// (refl::Options). Throws std::runtime_error on failure, as refl::write does.
+template <class SpotT, class PixelT, class OptionsT>
+void write_refl(const std::string &path, const std::vector<SpotT> &spots,
+                const std::vector<PixelT> &pixels, std::size_t width, const OptionsT &options) {
+  static_assert(sizeof(SpotT) == sizeof(sf_spot) && std::is_trivially_copyable<SpotT>::value,
+                "Spot must have the reference's 104-byte layout");
+  static_assert(sizeof(PixelT) == sizeof(sf_pixel) && std::is_trivially_copyable<PixelT>::value,
+                "Pixel must have the reference's 12-byte layout");
+  sf_refl_options o;
+  o.panel = options.panel;
+  o.id = options.id;
+  o.shoeboxes = options.shoeboxes ? 1 : 0;
+  o.identifier = options.identifier.c_str();
+  const int status = sf_refl_write(path.c_str(), reinterpret_cast<const sf_spot *>(spots.data()),
+                                   spots.size(),
+                                   reinterpret_cast<const sf_pixel *>(pixels.data()),
+                                   pixels.size(), width, &o);
+  if (status != 0)
+    throw std::runtime_error("refl::write " + path + ": " + sf_last_error());
+}
+
 } // namespace spotfinder_b200
 
 #endif // SPOTFINDER_B200_HPP

@@ -125,7 +125,8 @@ def ref_lib():
         lib.ref_labeller_pixels.argtypes = [_P, _P, _S]
         lib.ref_labeller_counts.argtypes = [_P, _P]
         lib.ref_spot_size.restype = _S
-        lib.ref_refl_write.argtypes = [ctypes.c_char_p, _P, _S, ctypes.c_char_p, ctypes.c_int]
+        lib.ref_refl_write.argtypes = [ctypes.c_char_p, _P, _S, ctypes.c_char_p, ctypes.c_int,
+                                       ctypes.c_int]
         assert lib.ref_spot_size() == SPOT.itemsize
         _ref = lib
     return _ref
@@ -247,11 +248,12 @@ class Labeller:
             live = lib.sfo_lab_live(self.handle)
         return Grouped(spots, pixels, dict(zip(COUNT_NAMES, (int(c) for c in counts))), int(live))
 
-    def write_refl(self, path: str, identifier: str = "", shoeboxes: bool = True) -> None:
+    def write_refl(self, path: str, identifier: str = "", shoeboxes: bool = True,
+                   experiment_id: int = 0) -> None:
         if not self.use_ref:
             raise RuntimeError("only the reference labeller writes .refl files")
         status = self.lib.ref_refl_write(path.encode(), self.handle, self.width,
-                                         identifier.encode(), int(shoeboxes))
+                                         identifier.encode(), int(shoeboxes), experiment_id)
         if status != 0:
             raise RuntimeError(self.lib.ref_last_error().decode())
 

@@ -160,12 +160,13 @@ void ref_labeller_counts(void *handle, std::uint64_t *out) {
 std::size_t ref_spot_size() { return sizeof(dials_spots::Spot); }
 
 int ref_refl_write(const char *path, void *handle, std::size_t width,
-                   const char *identifier, int shoeboxes) {
+                   const char *identifier, int shoeboxes, int id) {
   try {
     const auto *labeller = static_cast<dials_spots::Labeller *>(handle);
     refl::Options options;
     options.identifier = identifier == nullptr ? "" : identifier;
     options.shoeboxes = shoeboxes != 0;
+    options.id = id;
     refl::write(path, labeller->spots(), labeller->pixels(), width, options);
     return 0;
   } catch (const std::exception &error) {

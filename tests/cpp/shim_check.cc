@@ -6,9 +6,10 @@
 //       available=<0|1> backend=<...> stage0=<window> stage2=<window>
 //   shim_check find16|find32 H W image.raw out.raw
 //       out.raw: int32 status, uint64 count, count x 16-byte SignalPixel
-//   shim_check series16 NF H W Z0 TWO_D frames.raw spots.raw pixels.raw counts.raw
+//   shim_check series16 NF H W Z0 TWO_D frames.raw spots.raw pixels.raw counts.raw [out.refl]
 //       gpu::find<uint16_t> on each frame, then Labeller::add(Z0 + f); finish.
-//       counts.raw: six uint64 counts, then uint64 live
+//       counts.raw: six uint64 counts, then uint64 live; with out.refl also
+//       write_refl(identifier "golden", shoeboxes), as find_spots.cc does
 //   shim_check threads16 H W NTHREADS ROUNDS image.raw
 //       every thread runs gpu::find on the frame ROUNDS times; exit 0 if all
 //       lists are equal to the first
@@ -49,6 +50,12 @@ struct Counts {
   std::uint64_t signal_pixels = 0, groups = 0, too_small = 0, too_large = 0, separated = 0,
                 accepted = 0;
 };
+struct ReflOptions {
+  std::size_t panel = 0;
+  int id = 0;
+  std::string identifier;
+  bool shoeboxes = true;
+};
 struct Options {
   std::size_t min_spot_size = 3;
   std::size_t max_spot_size = 1000;
@@ -85,7 +92,7 @@ template <class T> int cmd_find(std::size_t h, std::size_t w, const char *in, co
 
 int cmd_series(int nf, std::size_t h, std::size_t w, std::int64_t z0, bool two_d,
                const char *in, const char *spots_out, const char *pixels_out,
-               const char *counts_out) {
+               const char *counts_out, const char *refl_out) {
   const std::vector<std::uint16_t> frames = read_raw<std::uint16_t>(in, nf * h * w);
   Options opt;
   opt.two_d = two_d;
@@ -117,6 +124,11 @@ int cmd_series(int nf, std::size_t h, std::size_t w, std::int64_t z0, bool two_d
   const std::uint64_t live = labeller.live();
   write_raw(counts_out, &c, sizeof(c));
   write_raw(counts_out, &live, 8, true);
+  if (refl_out) {
+    ReflOptions ro;
+    ro.identifier = "golden";
+    spotfinder_b200::write_refl(refl_out, spots, pixels, w, ro);
+  }
   return 0;
 }
 
@@ -181,10 +193,11 @@ int main(int argc, char **argv) {
       return cmd == "find16" ? cmd_find<std::uint16_t>(h, w, argv[4], argv[5])
                              : cmd_find<std::uint32_t>(h, w, argv[4], argv[5]);
     }
-    if (cmd == "series16" && argc == 11)
+    if (cmd == "series16" && (argc == 11 || argc == 12))
       return cmd_series(std::atoi(argv[2]), std::strtoull(argv[3], nullptr, 10),
                         std::strtoull(argv[4], nullptr, 10), std::strtoll(argv[5], nullptr, 10),
-                        std::atoi(argv[6]) != 0, argv[7], argv[8], argv[9], argv[10]);
+                        std::atoi(argv[6]) != 0, argv[7], argv[8], argv[9], argv[10],
+                        argc == 12 ? argv[11] : nullptr);
     if (cmd == "threads16" && argc == 7)
       return cmd_threads(std::strtoull(argv[2], nullptr, 10),
                          std::strtoull(argv[3], nullptr, 10), std::atoi(argv[4]),

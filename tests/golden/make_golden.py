@@ -22,6 +22,8 @@ Fixtures:
                      Labeller's spots, pixels and counts in 3D and in 2D.
   refl_small.refl    the reference refl::write of the 3D small-series spots
                      with shoeboxes, identifier "golden".
+  refl_small_2d.refl the same for the 2D grouping, no identifier.
+  refl_small_noshoebox.refl  the 3D spots without the shoebox column, id 3.
 """
 
 from __future__ import annotations
@@ -129,10 +131,33 @@ def small_series():
     np.savez_compressed(os.path.join(HERE, "small_series.npz"), **data)
 
 
+def refl_variants():
+    """refl::write with the other option branches: 2D spots with an empty
+    identifier map, and 3D spots without shoeboxes under experiment id 3."""
+    g = np.load(os.path.join(HERE, "small_series.npz"))
+    h, w = g["frames"].shape[1:]
+    signals = [np.ascontiguousarray(g["signal"][a:b]).view(O.SIGNAL_PIXEL).reshape(-1)
+               for a, b in zip(g["signal_offsets"][:-1], g["signal_offsets"][1:])]
+    for name, two_d, ident, ident_id, shoeboxes in (
+            ("refl_small_2d.refl", True, "", 0, True),
+            ("refl_small_noshoebox.refl", False, "golden-3", 3, False)):
+        lab = O.Labeller(h, w, two_d=two_d, use_ref=True)
+        for z, sig in enumerate(signals):
+            lab.add(z, sig)
+        lab.finish()
+        lab.write_refl(os.path.join(HERE, name), identifier=ident, shoeboxes=shoeboxes,
+                       experiment_id=ident_id)
+        print(name, len(lab.result().spots))
+
+
 if __name__ == "__main__":
     if not O.ref_available():
         sys.exit("oracle/_ref/libref.so is missing: run `make -C oracle ref` where the "
                  "reference tree is present")
+    if sys.argv[1:] == ["refl"]:
+        refl_variants()
+        sys.exit(0)
     threshold_u16()
     threshold_u32()
     small_series()
+    refl_variants()

@@ -114,7 +114,7 @@ def test_series_through_the_facade(tmp_path, two_d):
     nf, h, w = frames.shape
     frames.tofile(tmp_path / "frames.raw")
     run("series16", nf, h, w, 0, int(two_d), tmp_path / "frames.raw", tmp_path / "spots.raw",
-        tmp_path / "pixels.raw", tmp_path / "counts.raw")
+        tmp_path / "pixels.raw", tmp_path / "counts.raw", tmp_path / "strong.refl")
     tag = "2d" if two_d else "3d"
     spots = np.fromfile(tmp_path / "spots.raw", O.SPOT)
     pixels = np.fromfile(tmp_path / "pixels.raw", O.PIXEL)
@@ -123,6 +123,9 @@ def test_series_through_the_facade(tmp_path, two_d):
     assert pixels.tobytes() == as_records(g[f"pixels_{tag}"], O.PIXEL).tobytes()
     assert list(counts[:6]) == list(g[f"counts_{tag}"])
     assert counts[6] == 0  # finish() leaves nothing live
+    if not two_d:  # the reference's refl::write of the same spots, identifier "golden"
+        assert (tmp_path / "strong.refl").read_bytes() == \
+            open(os.path.join(ROOT, "tests", "golden", "refl_small.refl"), "rb").read()
 
 
 @pytest.mark.gpu
