@@ -104,6 +104,12 @@ SIGNATURES = {
     "sf_engine_profile": (_I, [_P, _I]),
     "sf_engine_stage_totals": (_I, [_P, _P]),
     "sf_engine_enable_grouping": (_I, [_P, _P, ctypes.c_int64, ctypes.c_uint64]),
+    "sf_engine_nseries": (_I, [_P]),
+    "sf_engine_series_shape": (_I, [_P, _I, ctypes.POINTER(ctypes.c_int32),
+                                    ctypes.POINTER(ctypes.c_int32)]),
+    "sf_engine_series_counts": (_I, [_P, _I, _P, ctypes.POINTER(ctypes.c_uint64)]),
+    "sf_engine_series_spots": (_I, [_P, _I, _P, _S, ctypes.POINTER(_S)]),
+    "sf_engine_series_pixels": (_I, [_P, _I, _P, _S, ctypes.POINTER(_S)]),
     "sf_engine_group_counts": (_I, [_P, _P, ctypes.POINTER(ctypes.c_uint64)]),
     "sf_engine_spots": (_I, [_P, _P, _S, ctypes.POINTER(_S)]),
     "sf_engine_pixels": (_I, [_P, _P, _S, ctypes.POINTER(_S)]),

@@ -41,11 +41,18 @@ struct Engine {
   std::vector<cudaEvent_t> ring;
   int ring_used = 0;
   uint32_t *pinned = nullptr;
-  // Grouping, when enabled: the labeller and the device copies of each
-  // frame's list offset and capacity.
-  std::unique_ptr<DeviceLabeller> lab;
-  uint64_t *d_offs = nullptr;
-  uint32_t *d_caps = nullptr;
+  // Grouping, when enabled: frames of one shape are one series, with its
+  // own labeller and the device copies of its frames' list offsets,
+  // capacities and plan frame numbers.
+  struct Series {
+    std::unique_ptr<DeviceLabeller> lab;
+    uint64_t *d_offs = nullptr;
+    uint32_t *d_caps = nullptr;
+    int32_t *d_map = nullptr;
+    int nframes = 0;
+    int32_t height = 0, width = 0;
+  };
+  std::vector<Series> series;
   int parity = 0;
   LabelScalars *host_sc = nullptr;
 
@@ -57,9 +64,12 @@ struct Engine {
     for (cudaGraphExec_t g : graphs)
       if (g)
         cudaGraphExecDestroy(g);
-    lab.reset();
-    cudaFree(d_offs);
-    cudaFree(d_caps);
+    for (Series &se : series) {
+      se.lab.reset();
+      cudaFree(se.d_offs);
+      cudaFree(se.d_caps);
+      cudaFree(se.d_map);
+    }
     if (host_sc)
       cudaFreeHost(host_sc);
     for (cudaEvent_t e : uploaded)
@@ -94,9 +104,9 @@ struct Engine {
     plan->enqueue(slot, compute, b);
     if (c)
       check(cudaEventRecord(c, compute), "cudaEventRecord");
-    if (lab)
-      lab->enqueue(plan->nframes(), plan->out(slot), d_offs, plan->frame_count(slot), d_caps,
-                   false, compute);
+    for (Series &se : series)
+      se.lab->enqueue(se.nframes, plan->out(slot), se.d_offs, plan->frame_count(slot), se.d_map,
+                      se.d_caps, false, compute);
   }
 
   void enqueue_run(int slot, cudaEvent_t a, cudaEvent_t b, cudaEvent_t c, cudaEvent_t d) {
@@ -120,8 +130,9 @@ struct Engine {
         const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
         cudaGraphDestroy(g);
         check(e, "instantiating the graph");
-      } else if (lab) {
-        lab->note_replayed(); // the captured run flips the live buffers too
+      } else {
+        for (Series &se : series)
+          se.lab->note_replayed(); // the captured run flips the live buffers too
       }
       check(cudaGraphLaunch(exec, compute), "launching the graph");
     } else {
@@ -129,7 +140,7 @@ struct Engine {
     }
     if (d)
       check(cudaEventRecord(d, compute), "cudaEventRecord");
-    if (lab)
+    if (!series.empty())
       parity ^= 1;
   }
 
@@ -149,40 +160,70 @@ struct Engine {
     check(cudaEventRecord(consumed[slot], compute), "cudaEventRecord");
   }
 
+  // Frames of one shape are the consecutive frames of one series, numbered
+  // from first_frame in their order within the batch and advancing run by
+  // run; each series is grouped by its own labeller, in the run's stream.
   void enable_grouping(const GroupOptions &opt, int64_t first_frame, uint64_t carry_cap) {
-    if (lab)
+    if (!series.empty())
       throw std::invalid_argument("grouping is already enabled");
     const int nf = plan->nframes();
-    int32_t h = plan->shape(0).height, w = plan->shape(0).width;
-    for (int f = 1; f < nf; f++)
-      if (plan->shape(f).height != h || plan->shape(f).width != w)
-        throw std::invalid_argument("grouping needs frames of one shape");
-    std::vector<uint64_t> offs(nf);
-    std::vector<uint32_t> caps(nf);
-    uint64_t total = 0, biggest = 0;
+    std::vector<std::vector<int32_t>> members;
     for (int f = 0; f < nf; f++) {
-      offs[f] = plan->out_base(f);
-      caps[f] = plan->capacity(f);
-      total += caps[f];
-      biggest = std::max<uint64_t>(biggest, caps[f]);
+      size_t k = 0;
+      while (k < series.size() && (series[k].height != plan->shape(f).height ||
+                                   series[k].width != plan->shape(f).width))
+        k++;
+      if (k == series.size()) {
+        series.emplace_back();
+        series.back().height = plan->shape(f).height;
+        series.back().width = plan->shape(f).width;
+        members.emplace_back();
+      }
+      members[k].push_back(f);
     }
-    check(cudaMalloc(&d_offs, nf * sizeof(uint64_t)), "cudaMalloc");
-    check(cudaMalloc(&d_caps, nf * sizeof(uint32_t)), "cudaMalloc");
-    check(cudaMemcpy(d_offs, offs.data(), nf * sizeof(uint64_t), cudaMemcpyHostToDevice), "copy");
-    check(cudaMemcpy(d_caps, caps.data(), nf * sizeof(uint32_t), cudaMemcpyHostToDevice), "copy");
     check(cudaMallocHost(&host_sc, sizeof(LabelScalars)), "cudaMallocHost");
-    lab = std::make_unique<DeviceLabeller>(h, w, opt);
-    lab->reserve(total, nf, carry_cap ? carry_cap : 2 * biggest + (1u << 20));
-    lab->set_next_frame(first_frame, compute);
+    for (size_t k = 0; k < series.size(); k++) {
+      Series &se = series[k];
+      const std::vector<int32_t> &fs = members[k];
+      se.nframes = static_cast<int>(fs.size());
+      std::vector<uint64_t> offs;
+      std::vector<uint32_t> caps;
+      uint64_t total = 0, biggest = 0;
+      for (int32_t f : fs) {
+        offs.push_back(plan->out_base(f));
+        caps.push_back(plan->capacity(f));
+        total += plan->capacity(f);
+        biggest = std::max<uint64_t>(biggest, plan->capacity(f));
+      }
+      const size_t n = fs.size();
+      check(cudaMalloc(&se.d_offs, n * sizeof(uint64_t)), "cudaMalloc");
+      check(cudaMalloc(&se.d_caps, n * sizeof(uint32_t)), "cudaMalloc");
+      check(cudaMalloc(&se.d_map, n * sizeof(int32_t)), "cudaMalloc");
+      check(cudaMemcpy(se.d_offs, offs.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice),
+            "copy");
+      check(cudaMemcpy(se.d_caps, caps.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice),
+            "copy");
+      check(cudaMemcpy(se.d_map, fs.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice), "copy");
+      se.lab = std::make_unique<DeviceLabeller>(se.height, se.width, opt);
+      se.lab->reserve(total, se.nframes, carry_cap ? carry_cap : 2 * biggest + (1u << 20));
+      se.lab->set_next_frame(first_frame, compute);
+    }
     check(cudaStreamSynchronize(compute), "cudaStreamSynchronize");
     parity = 0;
   }
 
-  const LabelScalars &group_state() {
-    if (!lab)
+  Series &series_at(int k) {
+    if (series.empty())
       throw std::invalid_argument("grouping is not enabled");
-    check(cudaMemcpyAsync(host_sc, lab->scalars(), sizeof(LabelScalars), cudaMemcpyDeviceToHost,
-                          compute),
+    if (k < 0 || k >= static_cast<int>(series.size()))
+      throw std::out_of_range("series out of range");
+    return series[k];
+  }
+
+  const LabelScalars &group_state(int k) {
+    Series &se = series_at(k);
+    check(cudaMemcpyAsync(host_sc, se.lab->scalars(), sizeof(LabelScalars),
+                          cudaMemcpyDeviceToHost, compute),
           "reading the grouping state");
     check(cudaStreamSynchronize(compute), "cudaStreamSynchronize");
     if (host_sc->status != kLabelOk)
@@ -467,11 +508,28 @@ int sf_engine_enable_grouping(sf_engine *engine, const sf_group_options *options
   });
 }
 
-int sf_engine_group_counts(sf_engine *engine, sf_counts *out, uint64_t *live) {
+int sf_engine_nseries(sf_engine *engine) {
+  if (!engine)
+    return -1;
+  return static_cast<int>(reinterpret_cast<Engine *>(engine)->series.size());
+}
+
+int sf_engine_series_shape(sf_engine *engine, int series, int32_t *height, int32_t *width) {
+  return guarded([&] {
+    if (!engine || !height || !width)
+      return -1;
+    const Engine::Series &se = reinterpret_cast<Engine *>(engine)->series_at(series);
+    *height = se.height;
+    *width = se.width;
+    return 0;
+  });
+}
+
+int sf_engine_series_counts(sf_engine *engine, int series, sf_counts *out, uint64_t *live) {
   return guarded([&] {
     if (!engine || !out)
       return -1;
-    const sf::LabelScalars &s = reinterpret_cast<Engine *>(engine)->group_state();
+    const sf::LabelScalars &s = reinterpret_cast<Engine *>(engine)->group_state(series);
     out->signal_pixels = s.signal_pixels;
     out->groups = s.groups;
     out->too_small = s.too_small;
@@ -484,38 +542,52 @@ int sf_engine_group_counts(sf_engine *engine, sf_counts *out, uint64_t *live) {
   });
 }
 
-int sf_engine_spots(sf_engine *engine, sf_spot *out, size_t capacity, size_t *n) {
+int sf_engine_series_spots(sf_engine *engine, int series, sf_spot *out, size_t capacity,
+                           size_t *n) {
   return guarded([&] {
     if (!engine || !n)
       return -1;
     Engine *e = reinterpret_cast<Engine *>(engine);
-    const sf::LabelScalars &s = e->group_state();
+    const sf::LabelScalars &s = e->group_state(series);
     *n = s.batch_spots;
     if (s.batch_spots > capacity)
       return -2;
     if (s.batch_spots)
-      sf::check(cudaMemcpy(out, e->lab->batch_spots(), s.batch_spots * sizeof(sf::Spot),
-                           cudaMemcpyDeviceToHost),
+      sf::check(cudaMemcpy(out, e->series[series].lab->batch_spots(),
+                           s.batch_spots * sizeof(sf::Spot), cudaMemcpyDeviceToHost),
                 "reading spots");
     return 0;
   });
 }
 
-int sf_engine_pixels(sf_engine *engine, sf_pixel *out, size_t capacity, size_t *n) {
+int sf_engine_series_pixels(sf_engine *engine, int series, sf_pixel *out, size_t capacity,
+                            size_t *n) {
   return guarded([&] {
     if (!engine || !n)
       return -1;
     Engine *e = reinterpret_cast<Engine *>(engine);
-    const sf::LabelScalars &s = e->group_state();
+    const sf::LabelScalars &s = e->group_state(series);
     *n = s.batch_pixels;
     if (s.batch_pixels > capacity)
       return -2;
     if (s.batch_pixels)
-      sf::check(cudaMemcpy(out, e->lab->batch_pixels(), s.batch_pixels * sizeof(sf::Pixel),
-                           cudaMemcpyDeviceToHost),
+      sf::check(cudaMemcpy(out, e->series[series].lab->batch_pixels(),
+                           s.batch_pixels * sizeof(sf::Pixel), cudaMemcpyDeviceToHost),
                 "reading spot pixels");
     return 0;
   });
+}
+
+int sf_engine_group_counts(sf_engine *engine, sf_counts *out, uint64_t *live) {
+  return sf_engine_series_counts(engine, 0, out, live);
+}
+
+int sf_engine_spots(sf_engine *engine, sf_spot *out, size_t capacity, size_t *n) {
+  return sf_engine_series_spots(engine, 0, out, capacity, n);
+}
+
+int sf_engine_pixels(sf_engine *engine, sf_pixel *out, size_t capacity, size_t *n) {
+  return sf_engine_series_pixels(engine, 0, out, capacity, n);
 }
 
 int sf_engine_finish(sf_engine *engine) {
@@ -523,10 +595,11 @@ int sf_engine_finish(sf_engine *engine) {
     if (!engine)
       return -1;
     Engine *e = reinterpret_cast<Engine *>(engine);
-    if (!e->lab)
+    if (e->series.empty())
       throw std::invalid_argument("grouping is not enabled");
-    e->lab->enqueue(0, e->plan->out(0), e->d_offs, e->plan->frame_count(0), e->d_caps, true,
-                    e->compute);
+    for (Engine::Series &se : e->series)
+      se.lab->enqueue(0, e->plan->out(0), se.d_offs, e->plan->frame_count(0), se.d_map,
+                      se.d_caps, true, e->compute);
     e->parity ^= 1;
     return 0;
   });

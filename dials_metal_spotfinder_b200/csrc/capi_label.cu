@@ -103,7 +103,7 @@ struct HostLabeller {
     const uint32_t m[2] = {static_cast<uint32_t>(n), static_cast<uint32_t>(n)};
     check(cudaMemcpyAsync(meta, m, sizeof(m), cudaMemcpyHostToDevice, stream), "copying counts");
     dev->set_next_frame(frame, stream);
-    dev->enqueue(1, list, offs, meta, meta + 1, false, stream);
+    dev->enqueue(1, list, offs, meta, nullptr, meta + 1, false, stream);
     collect();
     started = true;
     last = frame;
@@ -113,7 +113,7 @@ struct HostLabeller {
     if (!started)
       return;
     dev->reserve(1, 1, carry + 1);
-    dev->enqueue(0, list, offs, meta, meta + 1, true, stream);
+    dev->enqueue(0, list, offs, meta, nullptr, meta + 1, true, stream);
     collect();
   }
 };

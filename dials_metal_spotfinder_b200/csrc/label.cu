@@ -57,6 +57,7 @@ struct LabArgs {
   const SignalPixel *lists;
   const uint64_t *offs;
   const uint32_t *counts;
+  const int32_t *count_map; // frame f's count is counts[count_map[f]]; null: counts[f]
   const uint32_t *caps;
   int32_t *fr;
   uint32_t *ix, *val, *par;
@@ -175,7 +176,7 @@ __global__ void lab_setup(LabArgs a) {
   }
   uint64_t pos = carry;
   for (int f = 0; f < a.nframes; f++) {
-    uint32_t c = a.counts[f];
+    uint32_t c = a.counts[a.count_map ? a.count_map[f] : f];
     if (c > a.caps[f]) // an over-dense frame: its list holds only this many
       c = a.caps[f];
     if (pos + c > a.live_cap) {
@@ -1181,7 +1182,8 @@ void DeviceLabeller::set_next_frame(int64_t z, cudaStream_t s) {
 }
 
 void DeviceLabeller::enqueue(int nframes, const SignalPixel *lists, const uint64_t *offs,
-                             const uint32_t *counts, const uint32_t *caps, bool close_all,
+                             const uint32_t *counts, const int32_t *count_map,
+                             const uint32_t *caps, bool close_all,
                              cudaStream_t s) {
   if (nframes > frame_cap_)
     throw std::invalid_argument("more frames than the labeller was sized for");
@@ -1200,6 +1202,7 @@ void DeviceLabeller::enqueue(int nframes, const SignalPixel *lists, const uint64
   a.lists = lists;
   a.offs = offs;
   a.counts = counts;
+  a.count_map = count_map;
   a.caps = caps;
   const Live &cur = live_[cur_];
   const Live &nxt = live_[cur_ ^ 1];

@@ -81,11 +81,13 @@ public:
 
   // Enqueue one batch of `nframes` consecutive frames numbered from the
   // device-side batch_z0, which the batch then advances by nframes. Frame
-  // f's list is lists[offs[f] ...] with counts[f] entries, all in device
-  // memory. With close_all every component is finished, as the reference's
-  // finish() does; nframes may then be 0.
+  // f's list is lists[offs[f] ...] holding up to caps[f] records, with
+  // counts[count_map[f]] entries (counts[f] when count_map is null), all in
+  // device memory. With close_all every component is finished, as the
+  // reference's finish() does; nframes may then be 0.
   void enqueue(int nframes, const SignalPixel *lists, const uint64_t *offs,
-               const uint32_t *counts, const uint32_t *caps, bool close_all, cudaStream_t s);
+               const uint32_t *counts, const int32_t *count_map, const uint32_t *caps,
+               bool close_all, cudaStream_t s);
 
   // Sets batch_z0 for the next enqueue (an asynchronous copy from pinned
   // host memory; the labeller keeps the staging word until the next call).

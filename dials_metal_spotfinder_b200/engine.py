@@ -123,38 +123,51 @@ class Engine:
     # -- grouping inside each run ------------------------------------------
     def enable_grouping(self, first_frame: int = 0, min_spot_size=3, max_spot_size=1000,
                         max_separation=2.0, two_d=False, carry_capacity=0) -> None:
-        """Every run's frames are the next consecutive frames of one series;
-        they are grouped on the device right after their threshold (the
-        reference's Labeller::add per frame, src/dials_spots.cc:57-145)."""
+        """The batch's frames of one shape are one series; each run's frames of
+        a series are its next consecutive frames, grouped on the device right
+        after their threshold by that series' labeller (the reference's
+        Labeller::add per frame, src/dials_spots.cc:57-145)."""
         opt = GroupOptions(min_spot_size, max_spot_size, max_separation, int(two_d), 0)
         raise_for(lib.sf_engine_enable_grouping(self._h, ctypes.byref(opt), int(first_frame),
                                                 int(carry_capacity)), "enable_grouping")
 
-    def group_counts(self):
+    def nseries(self) -> int:
+        return int(lib.sf_engine_nseries(self._h))
+
+    def series_shape(self, series: int = 0):
+        h, w = ctypes.c_int32(0), ctypes.c_int32(0)
+        raise_for(lib.sf_engine_series_shape(self._h, series, ctypes.byref(h), ctypes.byref(w)),
+                  "series_shape")
+        return int(h.value), int(w.value)
+
+    def group_counts(self, series: int = 0):
         out = (ctypes.c_uint64 * 6)()
         live = ctypes.c_uint64(0)
-        raise_for(lib.sf_engine_group_counts(self._h, out, ctypes.byref(live)), "group_counts")
+        raise_for(lib.sf_engine_series_counts(self._h, series, out, ctypes.byref(live)),
+                  "group_counts")
         return dict(zip(COUNT_NAMES, (int(v) for v in out))), int(live.value)
 
-    def spots(self) -> np.ndarray:
-        """Spots finished by the last run (or by finish())."""
+    def spots(self, series: int = 0) -> np.ndarray:
+        """Spots of a series finished by the last run (or by finish())."""
         n = ctypes.c_size_t(0)
-        status = lib.sf_engine_spots(self._h, None, 0, ctypes.byref(n))
+        status = lib.sf_engine_series_spots(self._h, series, None, 0, ctypes.byref(n))
         if status not in (0, -2):
             raise_for(status, "spots")
         out = np.zeros(n.value, SPOT)
-        raise_for(lib.sf_engine_spots(self._h, out.ctypes.data if n.value else None, n.value,
-                                      ctypes.byref(n)), "spots")
+        raise_for(lib.sf_engine_series_spots(self._h, series,
+                                             out.ctypes.data if n.value else None, n.value,
+                                             ctypes.byref(n)), "spots")
         return out
 
-    def pixels(self) -> np.ndarray:
+    def pixels(self, series: int = 0) -> np.ndarray:
         n = ctypes.c_size_t(0)
-        status = lib.sf_engine_pixels(self._h, None, 0, ctypes.byref(n))
+        status = lib.sf_engine_series_pixels(self._h, series, None, 0, ctypes.byref(n))
         if status not in (0, -2):
             raise_for(status, "pixels")
         out = np.zeros(n.value, PIXEL)
-        raise_for(lib.sf_engine_pixels(self._h, out.ctypes.data if n.value else None, n.value,
-                                       ctypes.byref(n)), "pixels")
+        raise_for(lib.sf_engine_series_pixels(self._h, series,
+                                              out.ctypes.data if n.value else None, n.value,
+                                              ctypes.byref(n)), "pixels")
         return out
 
     def finish(self) -> None:

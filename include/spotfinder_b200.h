@@ -247,22 +247,38 @@ SF_API int sf_engine_elapsed(sf_engine *engine, int from, int to, float *ms);
 SF_API int sf_engine_profile(sf_engine *engine, int on);
 SF_API int sf_engine_stage_totals(sf_engine *engine, double out4[4]);
 
-/* Grouping inside every run (frames of one shape): each run's frames are
- * the next consecutive frames of one series starting at `first_frame`, and
- * go through sf_labeller's arithmetic on the device right after their
- * threshold, in the same stream (and graph). `carry_capacity` bounds the
- * pixels held open between runs (0: twice a frame's list capacity plus
- * 2^20); going past it makes the run report -3. */
+/* Grouping inside every run. The batch's frames of one shape form one
+ * series (several shapes: several series, e.g. concurrent detectors or
+ * interleaved stills runs); each run's frames of a series are that series'
+ * next consecutive frames, numbered from `first_frame`, and go through
+ * sf_labeller's arithmetic on the device right after their threshold, in
+ * the same stream (and graph), one labeller per series (the reference runs
+ * one dials_spots::Labeller per series, src/find_spots.cc:460-636).
+ * `carry_capacity` bounds the pixels a series holds open between runs (0:
+ * twice its biggest frame's list capacity plus 2^20); going past it makes
+ * the run report -3. Series are numbered in order of their first frame. */
 SF_API int sf_engine_enable_grouping(sf_engine *engine, const sf_group_options *options,
                                      int64_t first_frame, uint64_t carry_capacity);
-/* Running totals over the series and the pixels held open (waits). */
+/* Number of series (0 before grouping is enabled) and a series' shape. */
+SF_API int sf_engine_nseries(sf_engine *engine);
+SF_API int sf_engine_series_shape(sf_engine *engine, int series, int32_t *height,
+                                  int32_t *width);
+/* Running totals over a series and the pixels it holds open (waits). */
+SF_API int sf_engine_series_counts(sf_engine *engine, int series, sf_counts *out,
+                                   uint64_t *live);
+/* The spots, and their pixels, of a series finished by the last run
+ * (waits); -2 and *n set if `capacity` is too small. Spot::first counts from
+ * the series start. */
+SF_API int sf_engine_series_spots(sf_engine *engine, int series, sf_spot *out, size_t capacity,
+                                  size_t *n);
+SF_API int sf_engine_series_pixels(sf_engine *engine, int series, sf_pixel *out,
+                                   size_t capacity, size_t *n);
+/* The same for series 0 (a batch of one shape). */
 SF_API int sf_engine_group_counts(sf_engine *engine, sf_counts *out, uint64_t *live);
-/* The spots, and their pixels, finished by the last run (waits); -2 and *n
- * set if `capacity` is too small. Spot::first counts from the series start. */
 SF_API int sf_engine_spots(sf_engine *engine, sf_spot *out, size_t capacity, size_t *n);
 SF_API int sf_engine_pixels(sf_engine *engine, sf_pixel *out, size_t capacity, size_t *n);
-/* Close everything still open (Labeller::finish); its spots are then the
- * last run's. */
+/* Close everything still open in every series (Labeller::finish); its
+ * spots are then the last run's. */
 SF_API int sf_engine_finish(sf_engine *engine);
 
 #ifdef __cplusplus
