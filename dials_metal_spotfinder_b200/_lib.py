@@ -89,11 +89,15 @@ SIGNATURES = {
     "sf_labeller_spots": (_I, [_P, _P, _S]),
     "sf_labeller_pixels": (_I, [_P, _P, _S]),
     "sf_refl_write": (_I, [ctypes.c_char_p, _P, _S, _P, _S, _S, _P]),
+    "sf_chunk_bound": (_S, [_S, _S, _I]),
+    "sf_chunk_encode": (_I, [_I, _P, _S, _S, _I, _P, _S, ctypes.POINTER(_S)]),
+    "sf_chunk_decode": (_I, [_I, _P, _S, _S, _S, _I, _P]),
     "sf_engine_create": (_I, [_I, _I, _P, _P, _P, ctypes.POINTER(_P)]),
     "sf_engine_destroy": (None, [_P]),
     "sf_engine_info": (_I, [_P, _P]),
     "sf_engine_upload": (_I, [_P, _I, _I, _P]),
     "sf_engine_upload_device": (_I, [_P, _I, _I, _P, _S]),
+    "sf_engine_upload_chunk": (_I, [_P, _I, _I, _P, _S, _I]),
     "sf_engine_run": (_I, [_P, _I]),
     "sf_engine_use_graph": (_I, [_P, _I]),
     "sf_engine_synchronize": (_I, [_P]),

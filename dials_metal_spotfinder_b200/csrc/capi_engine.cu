@@ -14,6 +14,7 @@
 
 #include "../../include/spotfinder_b200.h"
 #include "sf_capi.hh"
+#include "sf_codec.hh"
 #include "sf_host.hh"
 #include "sf_label.hh"
 
@@ -55,6 +56,8 @@ struct Engine {
   std::vector<Series> series;
   int parity = 0;
   LabelScalars *host_sc = nullptr;
+  // Compressed uploads, decoded on the device in the copy stream.
+  DeviceChunkDecoder decoder;
 
   ~Engine() {
     if (compute)
@@ -248,9 +251,24 @@ struct Engine {
     check(cudaEventRecord(uploaded[slot], copy), "cudaEventRecord");
   }
 
+  void upload_chunk(int slot, int frame, const void *chunk, size_t nbytes, int algorithm) {
+    check_slot(slot);
+    check_frame(frame);
+    const ThresholdPlan::Shape &sh = plan->shape(frame);
+    const size_t eb = static_cast<size_t>(plan->elem_bytes());
+    const ChunkLayout L = parse_chunk(algorithm, static_cast<const uint8_t *>(chunk), nbytes,
+                                      static_cast<size_t>(sh.height) * sh.width, eb);
+    check(cudaStreamWaitEvent(copy, consumed[slot], 0), "ordering after the last run");
+    decoder.enqueue(static_cast<const uint8_t *>(chunk), nbytes, L, sh.height, sh.width,
+                    plan->frame_origin(slot, frame), plan->pitch() * eb, copy);
+    check(cudaEventRecord(uploaded[slot], copy), "cudaEventRecord");
+  }
+
   void synchronize() {
     check(cudaStreamSynchronize(copy), "cudaStreamSynchronize");
     check(cudaStreamSynchronize(compute), "cudaStreamSynchronize");
+    if (decoder.take_error())
+      throw DeviceError("an uploaded chunk held a malformed LZ4 block");
     for (int s = 0; s < plan->nslots(); s++) {
       int status = 0;
       check(cudaMemcpy(&status, plan->status(s), sizeof(int), cudaMemcpyDeviceToHost),
@@ -347,6 +365,16 @@ int sf_engine_upload_device(sf_engine *engine, int slot, int frame, const void *
     if (!engine || !device_image)
       return -1;
     reinterpret_cast<Engine *>(engine)->upload_device(slot, frame, device_image, pitch_bytes);
+    return 0;
+  });
+}
+
+int sf_engine_upload_chunk(sf_engine *engine, int slot, int frame, const void *chunk,
+                           size_t nbytes, int algorithm) {
+  return guarded([&] {
+    if (!engine || !chunk)
+      return -1;
+    reinterpret_cast<Engine *>(engine)->upload_chunk(slot, frame, chunk, nbytes, algorithm);
     return 0;
   });
 }

@@ -70,6 +70,14 @@ class Engine:
         raise_for(lib.sf_engine_upload_device(self._h, slot, frame, ptr, pitch_bytes),
                   "upload_device")
 
+    def upload_chunk(self, slot: int, frame: int, chunk: np.ndarray, algorithm="bslz4") -> None:
+        """A compressed frame (see chunk.py), decoded on the device into the
+        slot; keep `chunk` alive until the next synchronize()."""
+        from .chunk import algorithm_code
+        chunk = np.ascontiguousarray(chunk, dtype=np.uint8)
+        raise_for(lib.sf_engine_upload_chunk(self._h, slot, frame, chunk.ctypes.data, len(chunk),
+                                             algorithm_code(algorithm)), "upload_chunk")
+
     def run(self, slot: int = 0) -> None:
         raise_for(lib.sf_engine_run(self._h, slot), "run")
 

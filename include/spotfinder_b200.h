@@ -172,6 +172,26 @@ SF_API size_t sf_labeller_live(sf_labeller *labeller);
 SF_API int sf_labeller_spots(sf_labeller *labeller, sf_spot *out, size_t capacity);
 SF_API int sf_labeller_pixels(sf_labeller *labeller, sf_pixel *out, size_t capacity);
 
+/* ---- detector chunks: src/decompress.hh:14-31 (decompress::image) ------- *
+ *
+ * A frame as the HDF5 filters store it: SF_CHUNK_RAW (uncompressed),
+ * SF_CHUNK_LZ4 (the HDF5 LZ4 filter: 12-byte big-endian header of size and
+ * block size, then per block a 4-byte big-endian length and an LZ4 block)
+ * or SF_CHUNK_BSLZ4 (bitshuffle + LZ4, as Eiger detectors write: the same
+ * header, then per block of elements an LZ4 block of its bit transpose, the
+ * last elements mod 8 raw). Bitshuffle blocks of up to 16 KB are accepted.
+ * sf_chunk_encode writes one (8 KB blocks), as a detector or a replay source
+ * would; sf_chunk_decode is the host decoder. Both return -1 for bad
+ * arguments or a chunk that does not describe the frame (header size,
+ * framing, malformed LZ4), -2 (encode) if `capacity` is too small. */
+enum { SF_CHUNK_RAW = 0, SF_CHUNK_LZ4 = 1, SF_CHUNK_BSLZ4 = 2 };
+/* An upper bound on an encoded chunk's size. */
+SF_API size_t sf_chunk_bound(size_t height, size_t width, int elem_bytes);
+SF_API int sf_chunk_encode(int algorithm, const void *image, size_t height, size_t width,
+                           int elem_bytes, void *out, size_t capacity, size_t *written);
+SF_API int sf_chunk_decode(int algorithm, const void *chunk, size_t nbytes, size_t height,
+                           size_t width, int elem_bytes, void *image);
+
 /* ---- the reflection table: src/refl.hh:72-74 (refl::write) ------------- *
  *
  * Writes `spots` (with their pixels, `width` the frame width the labeller
@@ -224,6 +244,13 @@ SF_API int sf_engine_upload(sf_engine *engine, int slot, int frame, const void *
 /* The same from device memory with a row pitch in bytes. */
 SF_API int sf_engine_upload_device(sf_engine *engine, int slot, int frame,
                                    const void *device_image, size_t pitch_bytes);
+/* A compressed chunk (SF_CHUNK_*) of frame `frame`, decoded on the device
+ * into the slot: only the chunk's bytes cross PCIe. The framing is checked
+ * on the host first (-1 on a mismatch); a malformed LZ4 block found on the
+ * device makes the next synchronize report -3. Keep `chunk` alive and
+ * unchanged until the next synchronize. */
+SF_API int sf_engine_upload_chunk(sf_engine *engine, int slot, int frame, const void *chunk,
+                                  size_t nbytes, int algorithm);
 /* Enqueue the threshold of every frame of a slot, after its uploads. */
 SF_API int sf_engine_run(sf_engine *engine, int slot);
 /* Replay each slot's run from a CUDA graph captured on first use. */

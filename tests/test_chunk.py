@@ -1,0 +1,226 @@
+"""The detector chunk codec (sf_chunk_*; the reference's decompress::image,
+src/decompress.cc:85-134): HDF5 filter framing, LZ4 blocks and the
+bitshuffle transpose.
+
+The reference links the bitshuffle library and liblz4 for these, neither of
+which is vendored (its third_party/bitshuffle submodule is empty). The LZ4
+blocks are pinned against the system's liblz4 (LZ4_compress_default /
+LZ4_decompress_safe, called through its public API) where it is installed;
+the bit transpose against a numpy restatement of the published layout (bit
+k of byte j of element e at bit e mod 8 of byte e / 8 of row 8j + k).
+Host tests need no device; the device decoder's tests are marked gpu."""
+
+import ctypes
+import ctypes.util
+import struct
+
+import numpy as np
+import pytest
+
+from dials_metal_spotfinder_b200 import chunk as C
+from dials_metal_spotfinder_b200._lib import BadArgument
+
+
+def liblz4():
+    for name in ("lz4", "liblz4.so.1"):
+        path = ctypes.util.find_library(name) if name == "lz4" else name
+        if not path:
+            continue
+        try:
+            lib = ctypes.CDLL(path)
+        except OSError:
+            continue
+        lib.LZ4_compress_default.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int,
+                                             ctypes.c_int]
+        lib.LZ4_decompress_safe.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int,
+                                            ctypes.c_int]
+        return lib
+    return None
+
+
+LZ4 = liblz4()
+needs_liblz4 = pytest.mark.skipif(LZ4 is None, reason="liblz4 is not installed")
+
+
+def frames():
+    rng = np.random.default_rng(11)
+    out = []
+    for h, w in [(1, 1), (1, 7), (3, 5), (17, 31), (64, 128), (257, 511), (1062, 1028)]:
+        img = rng.poisson(1.5, (h, w)).astype(np.uint16)
+        img[rng.random((h, w)) < 0.01] = rng.integers(100, 60000)
+        if w > 10:
+            img[:, w // 3] = 0xFFFF  # a module gap
+        out.append(img)
+    big = rng.integers(0, 2 ** 32, (130, 77), dtype=np.uint64).astype(np.uint32)
+    out.append(big)
+    out.append(np.zeros((40, 40), np.uint32))
+    return out
+
+
+def split_blocks(raw, n_coded):
+    size, block = struct.unpack(">QI", raw[:12])
+    at, done, out = 12, 0, []
+    while done < n_coded:
+        (cs,) = struct.unpack(">I", raw[at:at + 4])
+        out.append(raw[at + 4:at + 4 + cs])
+        at += 4 + cs
+        done += min(block, n_coded - done)
+    return size, block, out, raw[at:]
+
+
+def bit_transpose(block: np.ndarray) -> bytes:
+    """The published bitshuffle layout of one block (numpy restatement)."""
+    n = len(block)
+    s = block.dtype.itemsize
+    b = block.view(np.uint8).reshape(n, s)                  # [element][byte]
+    bits = np.unpackbits(b, axis=1, bitorder="little")       # [element][8*byte + bit]
+    rows = bits.T.reshape(8 * s, n // 8, 8)                 # [row][group][element % 8]
+    return np.packbits(rows, axis=2, bitorder="little").reshape(-1).tobytes()
+
+
+@pytest.mark.parametrize("algorithm", ["raw", "lz4", "bslz4"])
+def test_round_trip(algorithm):
+    for img in frames():
+        chunk = C.encode(img, algorithm)
+        back = C.decode(chunk, img.shape, img.dtype, algorithm)
+        assert np.array_equal(back, img), (algorithm, img.shape, img.dtype)
+
+
+def test_synthetic_frames_compress():
+    from dials_metal_spotfinder_b200 import synth
+    img = synth.eiger_4m(frames=1).frame(0)
+    chunk = C.encode(img, "bslz4")
+    assert len(chunk) < img.nbytes / 2.5  # the high bit planes are almost all zero
+    assert np.array_equal(C.decode(chunk, img.shape), img)
+
+
+@needs_liblz4
+@pytest.mark.parametrize("algorithm", ["lz4", "bslz4"])
+def test_our_blocks_decode_with_liblz4(algorithm):
+    for img in frames():
+        n = img.size
+        s = img.dtype.itemsize
+        raw = bytes(C.encode(img, algorithm))
+        coded = (n - n % 8) * s if algorithm == "bslz4" else n * s
+        size, block, parts, rest = split_blocks(raw, coded)
+        assert size == img.nbytes and block == 8192
+        flat = img.reshape(-1)
+        at = 0
+        for part in parts:
+            nbytes = min(block, coded - at)
+            dst = ctypes.create_string_buffer(nbytes)
+            got = LZ4.LZ4_decompress_safe(part, dst, len(part), nbytes)
+            assert got == nbytes
+            if algorithm == "bslz4":
+                elems = flat[at // s:(at + nbytes) // s]
+                assert dst.raw == bit_transpose(elems)
+            else:
+                assert dst.raw == flat.view(np.uint8)[at:at + nbytes].tobytes()
+            at += nbytes
+        assert rest == flat.view(np.uint8)[coded:].tobytes()
+
+
+@needs_liblz4
+def test_liblz4_blocks_decode_with_ours():
+    rng = np.random.default_rng(5)
+    img = rng.poisson(0.7, (300, 333)).astype(np.uint16)
+    img[::7, ::5] = 4000
+    n, s = img.size, 2
+    flat = img.reshape(-1)
+    coded = (n - n % 8) * s
+    out = bytearray(struct.pack(">QI", img.nbytes, 8192))
+    for at in range(0, coded, 8192):
+        nbytes = min(8192, coded - at)
+        src = bit_transpose(flat[at // s:(at + nbytes) // s])
+        dst = ctypes.create_string_buffer(nbytes + nbytes // 255 + 64)
+        cs = LZ4.LZ4_compress_default(src, dst, nbytes, len(dst))
+        assert cs > 0
+        out += struct.pack(">I", cs) + dst.raw[:cs]
+    out += flat.view(np.uint8)[coded:].tobytes()
+    back = C.decode(np.frombuffer(bytes(out), np.uint8), img.shape, np.uint16, "bslz4")
+    assert np.array_equal(back, img)
+
+
+def test_malformed_chunks_are_refused():
+    rng = np.random.default_rng(2)
+    img = rng.poisson(2.0, (100, 90)).astype(np.uint16)
+    good = C.encode(img, "bslz4")
+    with pytest.raises(BadArgument):
+        C.decode(good[:-3], img.shape)                     # truncated
+    with pytest.raises(BadArgument):
+        C.decode(good, (100, 91))                          # header size mismatch
+    with pytest.raises(BadArgument):
+        C.decode(C.encode(img, "raw"), img.shape, algorithm="lz4")
+    bad = good.copy()
+    bad[16] ^= 0xF0                                        # a corrupted token
+    try:
+        back = C.decode(bad, img.shape)
+    except BadArgument:
+        pass
+    else:
+        assert not np.array_equal(back, img)
+    with pytest.raises(BadArgument):
+        C.decode(good, img.shape, algorithm=7)
+
+
+# -- the device decoder ------------------------------------------------------
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("algorithm", ["raw", "lz4", "bslz4"])
+def test_device_decode_feeds_the_engine(gpu_lib, algorithm):
+    from dials_metal_spotfinder_b200 import synth
+    from dials_metal_spotfinder_b200.engine import Engine
+    from oracle import oracle as O
+    shapes = [(2162, 2068), (257, 511), (1062, 1028)]
+    rng = np.random.default_rng(7)
+    imgs = [synth.eiger_4m(frames=1).frame(0)]
+    for h, w in shapes[1:]:
+        img = rng.poisson(1.2, (h, w)).astype(np.uint16)
+        img[rng.random((h, w)) < 0.003] = 5000
+        imgs.append(img)
+    chunks = [C.encode(img, algorithm) for img in imgs]
+    with Engine(shapes, np.uint16, slots=2) as eng:
+        for rep in range(2):  # reuse of the staging buffers
+            for f, ch in enumerate(chunks):
+                eng.upload_chunk(rep % 2, f, ch, algorithm)
+            eng.run(rep % 2)
+            eng.synchronize()
+            for f, img in enumerate(imgs):
+                assert eng.signal(rep % 2, f).tobytes() == O.dext(img)[1].tobytes()
+
+
+@pytest.mark.gpu
+def test_device_decode_u32(gpu_lib):
+    from dials_metal_spotfinder_b200.engine import Engine
+    from oracle import oracle as O
+    rng = np.random.default_rng(9)
+    img = rng.poisson(3.0, (333, 517)).astype(np.uint32)
+    img[rng.random(img.shape) < 0.002] = 2_000_000
+    with Engine([img.shape], np.uint32) as eng:
+        eng.upload_chunk(0, 0, C.encode(img, "bslz4"))
+        eng.run(0)
+        eng.synchronize()
+        assert eng.signal(0, 0).tobytes() == O.dext(img)[1].tobytes()
+
+
+@pytest.mark.gpu
+def test_device_reports_a_malformed_block(gpu_lib):
+    from dials_metal_spotfinder_b200._lib import DeviceError
+    from dials_metal_spotfinder_b200.engine import Engine
+    rng = np.random.default_rng(3)
+    img = rng.poisson(2.0, (256, 384)).astype(np.uint16)
+    good = C.encode(img, "bslz4")
+    size, block, parts, rest = split_blocks(bytes(good), img.nbytes)
+    # framing intact, first block's content replaced by a match whose offset
+    # reaches before the start of the output
+    first = bytes([0x0F, 0xFF, 0xFF]) + parts[0][3:]
+    bad = bytearray(good[:12]) + struct.pack(">I", len(first)) + first
+    bad += bytes(good[12 + 4 + len(parts[0]):])
+    with Engine([img.shape], np.uint16) as eng:
+        eng.upload_chunk(0, 0, np.frombuffer(bytes(bad), np.uint8))
+        eng.run(0)
+        with pytest.raises(DeviceError):
+            eng.synchronize()
+        eng.upload_chunk(0, 0, good)  # and the engine still works
+        eng.run(0)
+        eng.synchronize()
