@@ -92,6 +92,16 @@ SIGNATURES = {
     "sf_chunk_bound": (_S, [_S, _S, _I]),
     "sf_chunk_encode": (_I, [_I, _P, _S, _S, _I, _P, _S, ctypes.POINTER(_S)]),
     "sf_chunk_decode": (_I, [_I, _P, _S, _S, _S, _I, _P]),
+    "sf_server_create": (_I, [_P, ctypes.POINTER(_P)]),
+    "sf_server_destroy": (None, [_P]),
+    "sf_server_open": (_I, [_P, _S, _S, _I, _P, ctypes.c_int64, ctypes.POINTER(_I)]),
+    "sf_server_submit": (_I, [_P, _I, _P, _S, _I, ctypes.c_int64]),
+    "sf_server_close": (_I, [_P, _I]),
+    "sf_server_stats": (_I, [_P, _I, _P, _P]),
+    "sf_server_spots": (_I, [_P, _I, _P, _S, ctypes.POINTER(_S)]),
+    "sf_server_pixels": (_I, [_P, _I, _P, _S, ctypes.POINTER(_S)]),
+    "sf_server_signal_counts": (_I, [_P, _I, _P, _S, ctypes.POINTER(_S)]),
+    "sf_server_latencies": (_I, [_P, _I, _I, _P, _S, ctypes.POINTER(_S)]),
     "sf_engine_create": (_I, [_I, _I, _P, _P, _P, ctypes.POINTER(_P)]),
     "sf_engine_destroy": (None, [_P]),
     "sf_engine_info": (_I, [_P, _P]),
@@ -124,6 +134,11 @@ SIGNATURES = {
 class ReflOptions(ctypes.Structure):
     _fields_ = [("panel", ctypes.c_uint64), ("id", ctypes.c_int32), ("shoeboxes", ctypes.c_int32),
                 ("identifier", ctypes.c_char_p)]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget", ctypes.c_uint64), ("slots", ctypes.c_int32),
+                ("use_graph", ctypes.c_int32)]
 
 
 class EngineConfig(ctypes.Structure):

@@ -157,17 +157,18 @@ int64_t lz4_decompress(const uint8_t *in, size_t n, uint8_t *out, size_t cap) {
 
 // ---- bit transpose ----------------------------------------------------------
 
+// Eight elements at a time: byte j of elements 8g..8g+7 is one 64-bit word,
+// and its 8 x 8 bit transpose holds byte g of rows 8j..8j+7.
 void bit_transpose(const uint8_t *in, uint8_t *out, size_t n, size_t s) {
   const size_t row = n / 8;
-  std::memset(out, 0, n * s);
-  for (size_t e = 0; e < n; e++)
+  for (size_t g = 0; g < row; g++)
     for (size_t j = 0; j < s; j++) {
-      const uint8_t byte = in[e * s + j];
-      if (!byte)
-        continue;
+      uint64_t x = 0;
+      for (int i = 0; i < 8; i++)
+        x |= static_cast<uint64_t>(in[(8 * g + i) * s + j]) << (8 * i);
+      const uint64_t y = transpose8x8(x);
       for (int k = 0; k < 8; k++)
-        if (byte >> k & 1)
-          out[(8 * j + k) * row + e / 8] |= static_cast<uint8_t>(1u << (e % 8));
+        out[(8 * j + k) * row + g] = static_cast<uint8_t>(y >> (8 * k));
     }
 }
 

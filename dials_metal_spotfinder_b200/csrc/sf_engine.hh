@@ -1,0 +1,287 @@
+// The batched engine's state (capi_engine.cu holds the C entry points; the
+// serving loop in server.cu drives engines directly). Not part of the
+// public C ABI.
+#pragma once
+
+#include <algorithm>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "sf_codec.hh"
+#include "sf_host.hh"
+#include "sf_label.hh"
+
+namespace sf {
+
+constexpr int kMarks = 16;
+constexpr int kRingRuns = 4096;
+constexpr int kRunEvents = 4;
+
+struct Engine {
+  std::unique_ptr<ThresholdPlan> plan;
+  cudaStream_t compute = nullptr, copy = nullptr;
+  std::vector<cudaEvent_t> uploaded, consumed; // per slot
+  // Graphs per (slot, labeller parity): the labeller alternates between two
+  // live buffers, so a captured run is only valid for the parity it saw.
+  std::vector<cudaGraphExec_t> graphs;
+  bool use_graph = false;
+  cudaEvent_t marks[kMarks] = {};
+  // Profiling: per run, events before the threshold, between threshold and
+  // placement, after the placement and after the grouping.
+  bool profiling = false;
+  std::vector<cudaEvent_t> ring;
+  int ring_used = 0;
+  uint32_t *pinned = nullptr;
+  // Grouping, when enabled: frames of one shape are one series, with its
+  // own labeller and the device copies of its frames' list offsets,
+  // capacities and plan frame numbers.
+  struct Series {
+    std::unique_ptr<DeviceLabeller> lab;
+    uint64_t *d_offs = nullptr;
+    uint32_t *d_caps = nullptr;
+    int32_t *d_map = nullptr;
+    int nframes = 0;
+    int32_t height = 0, width = 0;
+  };
+  std::vector<Series> series;
+  int parity = 0;
+  LabelScalars *host_sc = nullptr;
+  // Compressed uploads, decoded on the device in the copy stream.
+  DeviceChunkDecoder decoder;
+  // Host callbacks in the run's stream, captured into its graphs too: after
+  // the signal lists are placed and after the grouping, each given its
+  // slot's argument. Set them before the first run.
+  cudaHostFn_t on_mask = nullptr, on_done = nullptr;
+  std::vector<void *> hook_args;
+
+  ~Engine() {
+    if (compute)
+      cudaStreamSynchronize(compute);
+    if (copy)
+      cudaStreamSynchronize(copy);
+    for (cudaGraphExec_t g : graphs)
+      if (g)
+        cudaGraphExecDestroy(g);
+    for (Series &se : series) {
+      se.lab.reset();
+      cudaFree(se.d_offs);
+      cudaFree(se.d_caps);
+      cudaFree(se.d_map);
+    }
+    if (host_sc)
+      cudaFreeHost(host_sc);
+    for (cudaEvent_t e : uploaded)
+      cudaEventDestroy(e);
+    for (cudaEvent_t e : consumed)
+      cudaEventDestroy(e);
+    for (cudaEvent_t e : marks)
+      if (e)
+        cudaEventDestroy(e);
+    for (cudaEvent_t e : ring)
+      cudaEventDestroy(e);
+    if (pinned)
+      cudaFreeHost(pinned);
+    plan.reset();
+    if (compute)
+      cudaStreamDestroy(compute);
+    if (copy)
+      cudaStreamDestroy(copy);
+  }
+
+  void check_slot(int slot) const {
+    if (slot < 0 || slot >= plan->nslots())
+      throw std::out_of_range("slot out of range");
+  }
+  void check_frame(int frame) const {
+    if (frame < 0 || frame >= plan->nframes())
+      throw std::out_of_range("frame out of range");
+  }
+
+  // Threshold, placement and (when enabled) grouping of one slot.
+  void enqueue_body(int slot, cudaEvent_t b, cudaEvent_t c) {
+    plan->enqueue(slot, compute, b);
+    if (c)
+      check(cudaEventRecord(c, compute), "cudaEventRecord");
+    if (on_mask)
+      check(cudaLaunchHostFunc(compute, on_mask, hook_args[slot]), "cudaLaunchHostFunc");
+    for (Series &se : series)
+      se.lab->enqueue(se.nframes, plan->out(slot), se.d_offs, plan->frame_count(slot), se.d_map,
+                      se.d_caps, false, compute);
+    if (on_done)
+      check(cudaLaunchHostFunc(compute, on_done, hook_args[slot]), "cudaLaunchHostFunc");
+  }
+
+  void enqueue_run(int slot, cudaEvent_t a, cudaEvent_t b, cudaEvent_t c, cudaEvent_t d) {
+    if (a)
+      check(cudaEventRecord(a, compute), "cudaEventRecord");
+    if (use_graph) {
+      cudaGraphExec_t &exec = graphs[2 * slot + parity];
+      if (!exec) {
+        cudaGraph_t g = nullptr;
+        check(cudaStreamBeginCapture(compute, cudaStreamCaptureModeThreadLocal),
+              "beginning graph capture");
+        try {
+          enqueue_body(slot, nullptr, nullptr);
+        } catch (...) {
+          cudaStreamEndCapture(compute, &g);
+          if (g)
+            cudaGraphDestroy(g);
+          throw;
+        }
+        check(cudaStreamEndCapture(compute, &g), "ending graph capture");
+        const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        check(e, "instantiating the graph");
+      } else {
+        for (Series &se : series)
+          se.lab->note_replayed(); // the captured run flips the live buffers too
+      }
+      check(cudaGraphLaunch(exec, compute), "launching the graph");
+    } else {
+      enqueue_body(slot, b, c);
+    }
+    if (d)
+      check(cudaEventRecord(d, compute), "cudaEventRecord");
+    if (!series.empty())
+      parity ^= 1;
+  }
+
+  void run(int slot) {
+    check_slot(slot);
+    check(cudaStreamWaitEvent(compute, uploaded[slot], 0), "ordering after the upload");
+    cudaEvent_t a = nullptr, b = nullptr, c = nullptr, d = nullptr;
+    if (profiling && ring_used < kRingRuns) {
+      cudaEvent_t *e = &ring[kRunEvents * ring_used];
+      a = e[0];
+      b = e[1];
+      c = e[2];
+      d = e[3];
+      ring_used++;
+    }
+    enqueue_run(slot, a, b, c, d);
+    check(cudaEventRecord(consumed[slot], compute), "cudaEventRecord");
+  }
+
+  // Frames of one shape are the consecutive frames of one series, numbered
+  // from first_frame in their order within the batch and advancing run by
+  // run; each series is grouped by its own labeller, in the run's stream.
+  void enable_grouping(const GroupOptions &opt, int64_t first_frame, uint64_t carry_cap) {
+    if (!series.empty())
+      throw std::invalid_argument("grouping is already enabled");
+    const int nf = plan->nframes();
+    std::vector<std::vector<int32_t>> members;
+    for (int f = 0; f < nf; f++) {
+      size_t k = 0;
+      while (k < series.size() && (series[k].height != plan->shape(f).height ||
+                                   series[k].width != plan->shape(f).width))
+        k++;
+      if (k == series.size()) {
+        series.emplace_back();
+        series.back().height = plan->shape(f).height;
+        series.back().width = plan->shape(f).width;
+        members.emplace_back();
+      }
+      members[k].push_back(f);
+    }
+    check(cudaMallocHost(&host_sc, sizeof(LabelScalars)), "cudaMallocHost");
+    for (size_t k = 0; k < series.size(); k++) {
+      Series &se = series[k];
+      const std::vector<int32_t> &fs = members[k];
+      se.nframes = static_cast<int>(fs.size());
+      std::vector<uint64_t> offs;
+      std::vector<uint32_t> caps;
+      uint64_t total = 0, biggest = 0;
+      for (int32_t f : fs) {
+        offs.push_back(plan->out_base(f));
+        caps.push_back(plan->capacity(f));
+        total += plan->capacity(f);
+        biggest = std::max<uint64_t>(biggest, plan->capacity(f));
+      }
+      const size_t n = fs.size();
+      check(cudaMalloc(&se.d_offs, n * sizeof(uint64_t)), "cudaMalloc");
+      check(cudaMalloc(&se.d_caps, n * sizeof(uint32_t)), "cudaMalloc");
+      check(cudaMalloc(&se.d_map, n * sizeof(int32_t)), "cudaMalloc");
+      check(cudaMemcpy(se.d_offs, offs.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice),
+            "copy");
+      check(cudaMemcpy(se.d_caps, caps.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice),
+            "copy");
+      check(cudaMemcpy(se.d_map, fs.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice), "copy");
+      se.lab = std::make_unique<DeviceLabeller>(se.height, se.width, opt);
+      se.lab->reserve(total, se.nframes, carry_cap ? carry_cap : 2 * biggest + (1u << 20));
+      se.lab->set_next_frame(first_frame, compute);
+    }
+    check(cudaStreamSynchronize(compute), "cudaStreamSynchronize");
+    parity = 0;
+  }
+
+  Series &series_at(int k) {
+    if (series.empty())
+      throw std::invalid_argument("grouping is not enabled");
+    if (k < 0 || k >= static_cast<int>(series.size()))
+      throw std::out_of_range("series out of range");
+    return series[k];
+  }
+
+  const LabelScalars &group_state(int k) {
+    Series &se = series_at(k);
+    check(cudaMemcpyAsync(host_sc, se.lab->scalars(), sizeof(LabelScalars),
+                          cudaMemcpyDeviceToHost, compute),
+          "reading the grouping state");
+    check(cudaStreamSynchronize(compute), "cudaStreamSynchronize");
+    if (host_sc->status != kLabelOk)
+      throw DeviceError("grouping capacity exceeded (status " + std::to_string(host_sc->status) +
+                        ")");
+    return *host_sc;
+  }
+
+  void upload(int slot, int frame, const void *host) {
+    check_slot(slot);
+    check_frame(frame);
+    check(cudaStreamWaitEvent(copy, consumed[slot], 0), "ordering after the last run");
+    plan->upload(slot, frame, host, copy);
+    check(cudaEventRecord(uploaded[slot], copy), "cudaEventRecord");
+  }
+
+  void upload_device(int slot, int frame, const void *dev, size_t pitch) {
+    check_slot(slot);
+    check_frame(frame);
+    check(cudaStreamWaitEvent(copy, consumed[slot], 0), "ordering after the last run");
+    plan->upload_device(slot, frame, dev, pitch, copy);
+    check(cudaEventRecord(uploaded[slot], copy), "cudaEventRecord");
+  }
+
+  void upload_chunk(int slot, int frame, const void *chunk, size_t nbytes, int algorithm) {
+    check_slot(slot);
+    check_frame(frame);
+    const ThresholdPlan::Shape &sh = plan->shape(frame);
+    const size_t eb = static_cast<size_t>(plan->elem_bytes());
+    const ChunkLayout L = parse_chunk(algorithm, static_cast<const uint8_t *>(chunk), nbytes,
+                                      static_cast<size_t>(sh.height) * sh.width, eb);
+    check(cudaStreamWaitEvent(copy, consumed[slot], 0), "ordering after the last run");
+    decoder.enqueue(static_cast<const uint8_t *>(chunk), nbytes, L, sh.height, sh.width,
+                    plan->frame_origin(slot, frame), plan->pitch() * eb, copy);
+    check(cudaEventRecord(uploaded[slot], copy), "cudaEventRecord");
+  }
+
+  void synchronize() {
+    check(cudaStreamSynchronize(copy), "cudaStreamSynchronize");
+    check(cudaStreamSynchronize(compute), "cudaStreamSynchronize");
+    if (decoder.take_error())
+      throw DeviceError("an uploaded chunk held a malformed LZ4 block");
+    for (int s = 0; s < plan->nslots(); s++) {
+      int status = 0;
+      check(cudaMemcpy(&status, plan->status(s), sizeof(int), cudaMemcpyDeviceToHost),
+            "reading the status");
+      if (status == kStatusTmaTimeout)
+        throw DeviceError("a TMA load did not complete in time");
+      if (status == kStatusSpinTimeout)
+        throw DeviceError("a device wait gave up");
+    }
+  }
+};
+
+std::unique_ptr<Engine> make_engine(int elem_bytes, const std::vector<ThresholdPlan::Shape> &shapes,
+                                    const PlanTuning &tuning, int slots);
+
+} // namespace sf

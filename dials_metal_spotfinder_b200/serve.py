@@ -1,0 +1,231 @@
+"""The serving loop (include/spotfinder_b200.h, sf_server_*): live series on
+one device, admitted by device-memory budget, frames submitted as detector
+chunks and decoded, thresholded and grouped on the device as they arrive,
+concurrent series overlapping on the device. Also a driver that replays
+streams at fixed frame rates and reports latency percentiles, and the plain
+per-frame form (host decode, sf_find per frame, labeller per frame) run on
+the same streams for comparison."""
+
+from __future__ import annotations
+
+import ctypes
+import threading
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from ._lib import (COUNT_NAMES, PIXEL, SPOT, GroupOptions, ServerConfig, lib, raise_for,
+                   require_device)
+from .chunk import algorithm_code
+
+
+class Busy(RuntimeError):
+    """sf_server_open -2: the device-memory budget cannot hold the series now."""
+
+
+class Server:
+    def __init__(self, hbm_budget: int = 0, slots: int = 3, use_graph: bool = True):
+        require_device()
+        cfg = ServerConfig(hbm_budget, slots, int(use_graph))
+        h = ctypes.c_void_p()
+        raise_for(lib.sf_server_create(ctypes.byref(cfg), ctypes.byref(h)), "sf_server_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.sf_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def open(self, shape, dtype=np.uint16, first_frame=0, min_spot_size=3, max_spot_size=1000,
+             max_separation=2.0, two_d=False) -> int:
+        opt = GroupOptions(min_spot_size, max_spot_size, max_separation, int(two_d), 0)
+        sid = ctypes.c_int(-1)
+        status = lib.sf_server_open(self._h, shape[0], shape[1], np.dtype(dtype).itemsize,
+                                    ctypes.byref(opt), first_frame, ctypes.byref(sid))
+        if status == -2:
+            raise Busy("the device-memory budget cannot hold this series now")
+        raise_for(status, "sf_server_open")
+        return sid.value
+
+    def submit(self, series: int, chunk: np.ndarray, algorithm="bslz4", timeout_s=1.0) -> bool:
+        """False if no slot freed up within the timeout (the frame is dropped)."""
+        status = lib.sf_server_submit(self._h, series, chunk.ctypes.data, len(chunk),
+                                      algorithm_code(algorithm), int(timeout_s * 1e6))
+        if status == -2:
+            return False
+        raise_for(status, "sf_server_submit")
+        return True
+
+    def finish(self, series: int) -> None:
+        raise_for(lib.sf_server_close(self._h, series), "sf_server_close")
+
+    def stats(self, series: int) -> dict:
+        c = (ctypes.c_uint64 * 6)()
+        o = (ctypes.c_uint64 * 4)()
+        raise_for(lib.sf_server_stats(self._h, series, c, o), "sf_server_stats")
+        d = dict(zip(COUNT_NAMES, (int(v) for v in c)))
+        d.update(frames_done=int(o[0]), dropped=int(o[1]), device_bytes=int(o[2]),
+                 closed=bool(o[3]))
+        return d
+
+    def _array(self, fn, series, dtype, *extra):
+        n = ctypes.c_size_t(0)
+        status = fn(self._h, series, *extra, None, 0, ctypes.byref(n))
+        if status not in (0, -2):
+            raise_for(status, fn.__name__)
+        out = np.zeros(n.value, dtype)
+        raise_for(fn(self._h, series, *extra, out.ctypes.data if n.value else None, n.value,
+                     ctypes.byref(n)), fn.__name__)
+        return out[: n.value]
+
+    def spots(self, series: int) -> np.ndarray:
+        return self._array(lib.sf_server_spots, series, SPOT)
+
+    def pixels(self, series: int) -> np.ndarray:
+        return self._array(lib.sf_server_pixels, series, PIXEL)
+
+    def signal_counts(self, series: int) -> np.ndarray:
+        return self._array(lib.sf_server_signal_counts, series, np.uint32)
+
+    def latencies_us(self, series: int, kind: str = "mask") -> np.ndarray:
+        k = {"mask": 0, "grouped": 1, "spot": 2}[kind]
+        return self._array(lib.sf_server_latencies, series, np.float64, k)
+
+
+@dataclass
+class Stream:
+    """A live series: `chunks` (pre-encoded frames, cycled) submitted at
+    `rate_hz` for `frames` frames."""
+    shape: tuple
+    chunks: list
+    rate_hz: float
+    frames: int
+    algorithm: str = "bslz4"
+    two_d: bool = False
+    results: dict = field(default_factory=dict)
+
+
+def percentiles(v):
+    v = np.asarray(v, dtype=np.float64)
+    if len(v) == 0:
+        return {"p50": None, "p99": None, "max": None}
+    return {"p50": float(np.percentile(v, 50)), "p99": float(np.percentile(v, 99)),
+            "max": float(v.max())}
+
+
+def drive(streams, hbm_budget=0, slots=3, use_graph=True):
+    """Replays every stream on its own thread at its frame rate through one
+    Server and returns per-stream results (latencies in ms)."""
+    out = []
+    with Server(hbm_budget=hbm_budget, slots=slots, use_graph=use_graph) as srv:
+        ids = [srv.open(s.shape, two_d=s.two_d) for s in streams]
+        late = [0] * len(streams)
+        t0 = time.perf_counter() + 0.05
+
+        def produce(k):
+            s = streams[k]
+            period = 1.0 / s.rate_hz
+            for i in range(s.frames):
+                due = t0 + i * period
+                while True:
+                    now = time.perf_counter()
+                    if now >= due:
+                        break
+                    time.sleep(min(due - now, 0.0005))
+                if time.perf_counter() - due > period:
+                    late[k] += 1
+                srv.submit(ids[k], s.chunks[i % len(s.chunks)], s.algorithm, timeout_s=period)
+
+        threads = [threading.Thread(target=produce, args=(k,)) for k in range(len(streams))]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        wall = time.perf_counter() - t0
+        for k, s in enumerate(streams):
+            srv.finish(ids[k])
+            st = srv.stats(ids[k])
+            out.append({
+                "shape": list(s.shape), "rate_hz": s.rate_hz, "frames": s.frames,
+                "frames_done": st["frames_done"], "dropped": st["dropped"],
+                "late_submits": late[k], "sustained_fps": st["frames_done"] / wall,
+                "frame_to_mask_ms": {k2: (v / 1e3 if v is not None else None) for k2, v in
+                                     percentiles(srv.latencies_us(ids[k], "mask")).items()},
+                "frame_to_grouped_ms": {k2: (v / 1e3 if v is not None else None) for k2, v in
+                                        percentiles(srv.latencies_us(ids[k], "grouped")).items()},
+                "frame_to_spot_ms": {k2: (v / 1e3 if v is not None else None) for k2, v in
+                                     percentiles(srv.latencies_us(ids[k], "spot")).items()},
+                "spots": int(st["accepted"]), "device_bytes": st["device_bytes"],
+            })
+    return out
+
+
+def drive_plain(streams):
+    """The plain per-frame form on the same streams: per frame, host decode,
+    sf_find_u16 (upload, threshold, copy back) and a device labeller add, on
+    one host thread per stream. Latencies in ms from each frame's due time."""
+    from . import chunk as C
+    from . import find
+    from .labeller import Labeller
+    out = []
+    t0 = time.perf_counter() + 0.05
+    results = [None] * len(streams)
+
+    def consume(k):
+        s = streams[k]
+        period = 1.0 / s.rate_hz
+        lab = Labeller(*s.shape, two_d=s.two_d)
+        mask, spot_lat = [], []
+        pending_due = []
+        backlog = 0
+        for i in range(s.frames):
+            due = t0 + i * period
+            while True:
+                now = time.perf_counter()
+                if now >= due:
+                    break
+                time.sleep(min(due - now, 0.0005))
+            img = C.decode(s.chunks[i % len(s.chunks)], s.shape, np.uint16, s.algorithm)
+            sig = find(img)
+            t_mask = time.perf_counter()
+            mask.append(t_mask - due)
+            before = lab.spots()
+            lab.add(i, sig)
+            after = lab.spots()
+            t_spot = time.perf_counter()
+            for sp in after[len(before):]:
+                last = int(sp["bbox"][5]) - 1
+                spot_lat.append(t_spot - (t0 + last * period))
+            pending_due.append(due)
+            backlog = max(backlog, int((time.perf_counter() - due) / period))
+        lab.finish()
+        lab.close()
+        results[k] = (mask, spot_lat, backlog)
+
+    threads = [threading.Thread(target=consume, args=(k,)) for k in range(len(streams))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    wall = time.perf_counter() - t0
+    for k, s in enumerate(streams):
+        mask, spot_lat, backlog = results[k]
+        out.append({
+            "shape": list(s.shape), "rate_hz": s.rate_hz, "frames": s.frames,
+            "sustained_fps": s.frames / wall, "max_backlog_frames": backlog,
+            "frame_to_mask_ms": {k2: (v * 1e3 if v is not None else None)
+                                 for k2, v in percentiles(mask).items()},
+            "frame_to_spot_ms": {k2: (v * 1e3 if v is not None else None)
+                                 for k2, v in percentiles(spot_lat).items()},
+        })
+    return out

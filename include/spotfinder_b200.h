@@ -308,6 +308,57 @@ SF_API int sf_engine_pixels(sf_engine *engine, sf_pixel *out, size_t capacity, s
  * spots are then the last run's. */
 SF_API int sf_engine_finish(sf_engine *engine);
 
+/* ---- serving: live series on one device ---------------------------------- *
+ *
+ * Replaces the reference's series queue and -j worker pool (src/series.hh:
+ * 66-83, src/queue.hh, src/find_spots.cc:472-591). Series are admitted while
+ * the device-memory budget holds them; each gets its own engine (chunks
+ * decoded on the device, threshold, placement and grouping per frame, graph
+ * replay), streams and worker thread, so concurrent series overlap on the
+ * device; frames are admitted into a series' slots as they free up, and the
+ * open components stay on the device between frames. A series' results are
+ * exactly what sf_find_* and sf_labeller_* give for it alone. */
+typedef struct sf_server sf_server;
+typedef struct sf_server_config {
+  uint64_t hbm_budget; /* device bytes for series; 0: free memory less 2 GiB */
+  int32_t slots;       /* frames in flight per series; 0: 3 */
+  int32_t use_graph;   /* replay each series' runs from CUDA graphs */
+} sf_server_config;
+
+SF_API int sf_server_create(const sf_server_config *config, sf_server **out);
+/* Stops every worker (after its queued frames) and frees everything. */
+SF_API void sf_server_destroy(sf_server *server);
+/* Admits a series of height x width frames of elem_bytes (2 or 4) pixels,
+ * grouped with `options`, numbered from first_frame. -2 if its device memory
+ * does not fit in what is left of the budget (retry after a close). */
+SF_API int sf_server_open(sf_server *server, size_t height, size_t width, int elem_bytes,
+                          const sf_group_options *options, int64_t first_frame, int *series);
+/* The series' next frame, as a chunk (SF_CHUNK_*), copied before return.
+ * Waits up to timeout_us for a free slot; -2 if none freed: the frame is
+ * dropped (its number is skipped, which closes the open components, as a
+ * gap in the numbering does). Latencies count from entry. */
+SF_API int sf_server_submit(sf_server *server, int series, const void *chunk, size_t nbytes,
+                            int algorithm, int64_t timeout_us);
+/* No more frames: processes what is queued, finishes the grouping and
+ * returns the series' device memory to the budget. Results stay readable. */
+SF_API int sf_server_close(sf_server *server, int series);
+/* Grouping counts and [frames done, frames dropped, device bytes, closed]. */
+SF_API int sf_server_stats(sf_server *server, int series, sf_counts *counts, uint64_t out4[4]);
+/* The series' spots and their pixels so far (Spot::first from its start). */
+SF_API int sf_server_spots(sf_server *server, int series, sf_spot *out, size_t capacity,
+                           size_t *n);
+SF_API int sf_server_pixels(sf_server *server, int series, sf_pixel *out, size_t capacity,
+                            size_t *n);
+/* Signal pixels per frame, by frame number (0 for a dropped frame). */
+SF_API int sf_server_signal_counts(sf_server *server, int series, uint32_t *out,
+                                   size_t capacity, size_t *n);
+/* Latencies in microseconds: kind 0, per finished frame, submit to its
+ * signal list placed on the device (frame-to-mask); kind 1, submit to its
+ * grouping done; kind 2, per spot, submit of the spot's last frame to its
+ * row on the host (frame-to-finalised-spot). */
+SF_API int sf_server_latencies(sf_server *server, int series, int kind, double *out,
+                               size_t capacity, size_t *n);
+
 #ifdef __cplusplus
 }
 #endif
