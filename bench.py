@@ -61,6 +61,11 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=4)
     ap.add_argument("--cpu-frames", type=int, default=8)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--serve-seconds", type=float, default=3.0,
+                    help="length of the two-stream serving replay (0: skip)")
+    ap.add_argument("--plain-seconds", type=float, default=0.5,
+                    help="length of the plain per-frame replay of the same streams")
+    ap.add_argument("--no-4m", action="store_true")
     return ap.parse_args()
 
 
@@ -364,6 +369,14 @@ def run_ours(args, ranks):
     if ranks.rank == 0:
         ref_gpu = reference_gpu_form(pool[0])
 
+    four_m = None
+    if ranks.rank == 0 and not args.no_4m:
+        four_m = batched_vs_plain_4m()
+
+    served = None
+    if ranks.rank == 0 and args.serve_seconds > 0:
+        served = serving(args.serve_seconds, args.plain_seconds, pool)
+
     cpu = None
     if ranks.rank == 0 and ranks.world == 1 and not args.no_cpu:
         n = max(2, args.cpu_frames)
@@ -408,11 +421,95 @@ def run_ours(args, ranks):
         "e2e": e2e,
         "plain_gpu": plain,
         "reference_gpu": ref_gpu,
+        "batched_vs_plain_4m": four_m,
+        "latency": ({"frame_to_mask_p99_ms": {
+                        name: r["frame_to_mask_ms"]["p99"]
+                        for name, r in zip(("4m_500hz", "16m_100hz"), served["served"])},
+                     "frame_to_spot_p99_ms": {
+                        name: r["frame_to_spot_ms"]["p99"]
+                        for name, r in zip(("4m_500hz", "16m_100hz"), served["served"])},
+                     "source": "serving"} if served else None),
+        "serving": served,
         "cpu_baseline": cpu,
     }
     eng.close()
     if ranks.rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def batched_vs_plain_4m(steps: int = 10):
+    """4M-shaped frames (2162 x 2068): the batched engine (16 frames per
+    launch, resident, with 3D grouping, graph replay) against the plain
+    per-frame form (sf_find_u16 per frame from pinned host memory) on the
+    same frames, frames/s each."""
+    import dials_metal_spotfinder_b200 as sf
+    from dials_metal_spotfinder_b200 import synth
+    from dials_metal_spotfinder_b200.engine import Engine
+    series = synth.eiger_4m(frames=32)
+    pool = [series.frame(f) for f in range(32)]
+    shape = pool[0].shape
+    F = 16
+    with Engine([shape] * F, np.uint16, slots=2) as eng:
+        eng.enable_grouping(first_frame=0)
+        for s in range(2):
+            for f in range(F):
+                eng.upload(s, f, pool[s * F + f])
+        eng.synchronize()
+        eng.use_graph(True)
+        for i in range(4):
+            eng.run(i % 2)
+        eng.synchronize()
+        eng.record(0)
+        for i in range(steps):
+            eng.run(i % 2)
+        eng.record(1)
+        eng.synchronize()
+        batched = F * steps / (eng.elapsed_ms(0, 1) / 1e3)
+    hb = sf.HostBuffer(shape, np.uint16)
+    hb.array[:] = pool[0]
+    for _ in range(3):
+        sf.find(hb.array)
+    n = 30
+    t0 = time.perf_counter()
+    for i in range(n):
+        sf.find(hb.array)
+    plain = n / (time.perf_counter() - t0)
+    hb.close()
+    return {"workload": "4M-shaped uint16 frames, 2162x2068", "unit": UNIT,
+            "batched": batched, "plain": plain, "ratio": batched / plain,
+            "batched_form": "engine, 16 frames per launch, resident, threshold + 3D grouping, "
+                            "graph replay, CUDA events",
+            "plain_form": "sf_find_u16 per frame from pinned host memory, threshold only, "
+                          "host wall clock"}
+
+
+def serving(seconds: float, plain_seconds: float, pool16):
+    """Two live streams on one device through the serving loop, frames as
+    bitshuffle/LZ4 chunks decoded on the device: 4M at 500 Hz and 16M at
+    100 Hz. Then the plain per-frame form (host decode, sf_find_u16,
+    labeller) on the same streams for plain_seconds."""
+    from dials_metal_spotfinder_b200 import chunk as C
+    from dials_metal_spotfinder_b200 import synth
+    from dials_metal_spotfinder_b200.serve import Stream, drive, drive_plain
+    # distinct frames cycled, longer than any reflection's z extent
+    n = min(24, len(pool16))
+    s4 = synth.eiger_4m(frames=n)
+    c4 = [C.encode(s4.frame(f), "bslz4") for f in range(n)]
+    c16 = [C.encode(f, "bslz4") for f in pool16[:n]]
+    raw4 = s4.height * s4.width * 2
+    raw16 = pool16[0].nbytes
+
+    def streams(sec):
+        return [Stream((s4.height, s4.width), c4, rate_hz=500.0, frames=max(1, int(500 * sec))),
+                Stream(pool16[0].shape, c16, rate_hz=100.0, frames=max(1, int(100 * sec)))]
+    out = {"streams": "4M (2162x2068) at 500 Hz and 16M (4362x4148) at 100 Hz, bslz4 chunks",
+           "compression": {"4m": raw4 / statistics.mean(len(c) for c in c4),
+                           "16m": raw16 / statistics.mean(len(c) for c in c16)},
+           "seconds": seconds, "served": drive(streams(seconds))}
+    if plain_seconds > 0:
+        out["plain_seconds"] = plain_seconds
+        out["plain"] = drive_plain(streams(plain_seconds))
+    return out
 
 
 def reference_gpu_form(frame):

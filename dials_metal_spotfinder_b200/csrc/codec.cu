@@ -149,8 +149,21 @@ int64_t lz4_decompress(const uint8_t *in, size_t n, uint8_t *out, size_t cap) {
     }
     if (ml > cap - op)
       return -1;
-    for (size_t i = 0; i < ml; i++, op++)
-      out[op] = out[op - off];
+    if (off >= ml) {
+      std::memcpy(out + op, out + op - off, ml);
+      op += ml;
+    } else {
+      // overlapping: the last `off` bytes repeat; copy in doubling runs
+      size_t done = 0, period = off;
+      while (done < ml) {
+        const size_t n = std::min(period, ml - done);
+        std::memcpy(out + op + done, out + op + done - period, n);
+        done += n;
+        if (period < 4096 && done >= period)
+          period *= 2; // the last 2*period bytes are also a whole number of periods
+      }
+      op += ml;
+    }
   }
   return static_cast<int64_t>(op);
 }

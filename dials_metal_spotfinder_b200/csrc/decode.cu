@@ -174,16 +174,13 @@ void DeviceChunkDecoder::enqueue(const uint8_t *chunk, size_t nbytes, const Chun
           "copying a frame to the device");
     return;
   }
-  if (!d_err_) {
-    check(cudaMalloc(&d_err_, sizeof(int)), "cudaMalloc");
-    check(cudaMemsetAsync(d_err_, 0, sizeof(int), s), "clearing the decode flag");
-    static bool configured = false;
-    if (!configured) {
-      check(cudaFuncSetAttribute(decode_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(kDecodeWarps * kMaxBlockBytes)),
-            "cudaFuncSetAttribute");
-      configured = true;
-    }
+  error_flag();
+  static bool configured = false; // setting it twice is harmless
+  if (!configured) {
+    check(cudaFuncSetAttribute(decode_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(kDecodeWarps * kMaxBlockBytes)),
+          "cudaFuncSetAttribute");
+    configured = true;
   }
   const size_t frame_bytes = height * row_bytes;
   const size_t nb = L.block_in.size();
@@ -215,6 +212,15 @@ void DeviceChunkDecoder::enqueue(const uint8_t *chunk, size_t nbytes, const Chun
   check(cudaMemcpy2DAsync(dst, dst_pitch, d_linear_, row_bytes, row_bytes, height,
                           cudaMemcpyDeviceToDevice, s),
         "copying the decoded frame");
+}
+
+int *DeviceChunkDecoder::error_flag() {
+  if (!d_err_) {
+    check(cudaMalloc(&d_err_, sizeof(int)), "cudaMalloc");
+    check(cudaMemset(d_err_, 0, sizeof(int)), "clearing the decode flag");
+    check(cudaStreamSynchronize(cudaStreamLegacy), "clearing the decode flag");
+  }
+  return d_err_;
 }
 
 bool DeviceChunkDecoder::take_error() {

@@ -3,8 +3,12 @@
 // from their chunks on the device), its own streams and its own worker
 // thread, so the device work of concurrent series overlaps. Frames are
 // admitted into the series' slots as they free up; the union-find frontier
-// and the open components stay on the device between frames, and each
-// frame's finished spots are copied out as soon as its run completes.
+// and the open components stay on the device between frames. The worker
+// never waits for the device: each run ends with a kernel that writes its
+// results (signal count, status, counts, the spots it finished and their
+// pixels) into the slot's page-locked, device-mapped sink, and a host
+// callback; a second thread per series collects the sinks in frame order
+// and frees the slots, so the next frames upload and run meanwhile.
 //
 // Latencies are taken on the host's steady clock from the moment a frame is
 // submitted: to its signal list being placed on the device (a host callback
@@ -39,15 +43,65 @@ int64_t now_ns() {
 
 struct ServerSeries;
 
+// What a run leaves for the host, in page-locked memory the device writes.
+struct SinkHeader {
+  uint32_t nsig;      // the frame's signal pixels
+  int32_t status;     // 0, or what failed (kSink* bits)
+  uint64_t nspots, npixels;
+  uint64_t counts[6]; // running grouping counts
+};
+enum : int32_t { kSinkPlan = 1, kSinkDecode = 2, kSinkLabel = 4, kSinkOverflow = 8 };
+
 struct SlotState {
+  ServerSeries *series = nullptr;
   std::atomic<int64_t> t_mask{0}, t_done{0};
+  SinkHeader *h_sink = nullptr; // host view
+  SinkHeader *d_sink = nullptr; // the same memory, device view
 };
 
 void CUDART_CB mark_mask(void *arg) {
   static_cast<SlotState *>(arg)->t_mask.store(now_ns(), std::memory_order_release);
 }
-void CUDART_CB mark_done(void *arg) {
-  static_cast<SlotState *>(arg)->t_done.store(now_ns(), std::memory_order_release);
+void CUDART_CB mark_done(void *arg);
+
+// One run's results to its sink: the header from one thread, the spots and
+// pixels by the grid, capped at the sink's capacity (kSinkOverflow beyond).
+__global__ void sink_results(const LabelScalars *sc, const Spot *spots, const Pixel *pixels,
+                             const uint32_t *frame_count, const int *plan_status,
+                             const int *decode_err, SinkHeader *sink, uint64_t cap_spots,
+                             uint64_t cap_pixels) {
+  const uint64_t ns = sc->batch_spots, np = sc->batch_pixels;
+  const uint64_t tid = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const uint64_t stride = static_cast<uint64_t>(gridDim.x) * blockDim.x;
+  if (tid == 0) {
+    int32_t st = 0;
+    if (*plan_status)
+      st |= kSinkPlan;
+    if (decode_err && *decode_err)
+      st |= kSinkDecode;
+    if (sc->status)
+      st |= kSinkLabel;
+    if (ns > cap_spots || np > cap_pixels)
+      st |= kSinkOverflow;
+    sink->nsig = frame_count[0];
+    sink->status = st;
+    sink->nspots = ns;
+    sink->npixels = np;
+    const uint64_t c[6] = {sc->signal_pixels, sc->groups, sc->too_small, sc->too_large,
+                           sc->separated, sc->accepted};
+    for (int i = 0; i < 6; i++)
+      sink->counts[i] = c[i];
+  }
+  if (ns > cap_spots || np > cap_pixels)
+    return;
+  uint64_t *spot_words = reinterpret_cast<uint64_t *>(sink + 1);
+  const uint64_t *src_spots = reinterpret_cast<const uint64_t *>(spots);
+  for (uint64_t i = tid; i < ns * (sizeof(Spot) / 8); i += stride)
+    spot_words[i] = src_spots[i];
+  uint32_t *pixel_words = reinterpret_cast<uint32_t *>(spot_words + cap_spots * (sizeof(Spot) / 8));
+  const uint32_t *src_pixels = reinterpret_cast<const uint32_t *>(pixels);
+  for (uint64_t i = tid; i < np * (sizeof(Pixel) / 4); i += stride)
+    pixel_words[i] = src_pixels[i];
 }
 
 struct Pending {
@@ -65,20 +119,25 @@ struct ServerSeries {
   std::unique_ptr<Engine> eng;
   uint64_t device_bytes = 0;
   size_t chunk_cap = 0;
-  std::vector<uint8_t *> staging; // pinned, one chunk per slot
+  uint64_t cap_spots = 0, cap_pixels = 0; // per sink
+  std::vector<uint8_t *> staging;         // pinned, one chunk per slot
+  std::vector<void *> sinks;              // page-locked, device-mapped, one per slot
   std::vector<std::unique_ptr<SlotState>> slot_state;
 
   std::mutex m;
   std::condition_variable cv;
+  std::mutex done_m; // only for the runs' completion callbacks
+  std::condition_variable done_cv;
   std::deque<int> free_slots;
-  std::deque<Pending> queue;
-  int64_t next_frame = 0; // the next frame number a submission gets
-  bool closing = false, done = false;
-  std::thread worker;
+  std::deque<Pending> queue;    // submitted, not yet uploaded
+  std::deque<Pending> inflight; // uploaded and running, in frame order
+  int64_t next_frame = 0;       // the next frame number a submission gets
+  bool closing = false, worker_idle = false, done = false;
+  std::thread worker, collector;
 
-  // results, under m
-  std::vector<Spot> spots;
-  std::vector<Pixel> pixels;
+  // results, under m; spots and pixels in one block per run
+  std::vector<std::vector<Spot>> spots;
+  std::vector<std::vector<Pixel>> pixels;
   std::vector<uint32_t> signal_counts;
   std::vector<int64_t> t_submit; // per frame number
   std::vector<double> lat_mask, lat_grouped, lat_spot;
@@ -90,8 +149,29 @@ struct ServerSeries {
     for (uint8_t *p : staging)
       if (p)
         cudaFreeHost(p);
+    for (void *p : sinks)
+      if (p)
+        cudaFreeHost(p);
   }
 };
+
+void CUDART_CB mark_done(void *arg) {
+  SlotState *st = static_cast<SlotState *>(arg);
+  st->t_done.store(now_ns(), std::memory_order_release);
+  std::lock_guard<std::mutex> g(st->series->done_m);
+  st->series->done_cv.notify_all();
+}
+
+void post_run_sink(Engine &e, int slot, void *arg) {
+  ServerSeries *se = static_cast<ServerSeries *>(arg);
+  DeviceLabeller &lab = *e.series[0].lab;
+  sink_results<<<64, 256, 0, e.compute>>>(lab.scalars(), lab.batch_spots(), lab.batch_pixels(),
+                                          e.plan->frame_count(slot), e.plan->status(slot),
+                                          e.decoder.error_flag(),
+                                          se->slot_state[slot]->d_sink, se->cap_spots,
+                                          se->cap_pixels);
+  check(cudaGetLastError(), "launching the result sink");
+}
 
 } // namespace
 
@@ -138,15 +218,33 @@ struct Server {
       used += se->device_bytes;
     }
     se->chunk_cap = sf_chunk_bound(h, w, eb);
+    // A run's spots and pixels: up to four frames' list capacities of
+    // pixels (a frame can close components that began frames earlier) and
+    // 256 Ki spots; a run that finishes more reports an overflow.
+    se->cap_pixels = std::max<uint64_t>(4 * (h * w * eb / 16), 1u << 16);
+    se->cap_spots = 1u << 18;
+    const size_t sink_bytes =
+        sizeof(SinkHeader) + se->cap_spots * sizeof(Spot) + se->cap_pixels * sizeof(Pixel);
     se->staging.assign(slots, nullptr);
+    se->sinks.assign(slots, nullptr);
     for (int s = 0; s < slots; s++) {
       check(cudaMallocHost(&se->staging[s], se->chunk_cap), "cudaMallocHost");
-      se->slot_state.push_back(std::make_unique<SlotState>());
-      se->eng->hook_args[s] = se->slot_state[s].get();
+      check(cudaHostAlloc(&se->sinks[s], sink_bytes, cudaHostAllocMapped), "cudaHostAlloc sink");
+      auto st = std::make_unique<SlotState>();
+      st->series = se.get();
+      st->h_sink = static_cast<SinkHeader *>(se->sinks[s]);
+      void *dev = nullptr;
+      check(cudaHostGetDevicePointer(&dev, se->sinks[s], 0), "cudaHostGetDevicePointer");
+      st->d_sink = static_cast<SinkHeader *>(dev);
+      se->eng->hook_args[s] = st.get();
+      se->slot_state.push_back(std::move(st));
       se->free_slots.push_back(s);
     }
+    se->eng->decoder.error_flag();
     se->eng->on_mask = mark_mask;
     se->eng->on_done = mark_done;
+    se->eng->post_run = post_run_sink;
+    se->eng->post_arg = se.get();
     se->eng->use_graph = use_graph;
     ServerSeries *raw = se.get();
     {
@@ -155,6 +253,7 @@ struct Server {
       series.push_back(std::move(se));
     }
     raw->worker = std::thread([this, raw] { work(*raw); });
+    raw->collector = std::thread([this, raw] { collect_loop(*raw); });
     *out = raw->id;
     return 0;
   }
@@ -189,7 +288,8 @@ struct Server {
     return 0;
   }
 
-  // One series' frames, in order: decode on the device, run, read back.
+  // One series' frames, in order: decode on the device and run, without
+  // waiting for the device; collect_loop takes the results.
   void work(ServerSeries &se) {
     cudaSetDevice(se.device);
     int64_t expected = 0; // the frame number the labeller expects next
@@ -198,8 +298,8 @@ struct Server {
         Pending p;
         {
           std::unique_lock<std::mutex> lk(se.m);
-          se.cv.wait(lk, [&] { return !se.queue.empty() || se.closing; });
-          if (se.queue.empty())
+          se.cv.wait(lk, [&] { return !se.queue.empty() || se.closing || !se.error.empty(); });
+          if (!se.error.empty() || se.queue.empty())
             break;
           p = se.queue.front();
           se.queue.pop_front();
@@ -215,45 +315,109 @@ struct Server {
         st.t_mask.store(0);
         st.t_done.store(0);
         e.upload_chunk(p.slot, 0, se.staging[p.slot], p.nbytes, p.algorithm);
+        {
+          std::lock_guard<std::mutex> g(se.m);
+          se.inflight.push_back(p);
+          se.cv.notify_all(); // the collector waits for this
+        }
         e.run(p.slot);
-        e.synchronize();
         expected++;
-        uint32_t nsig = 0;
-        check(cudaMemcpy(&nsig, e.plan->frame_count(p.slot), sizeof(uint32_t),
-                         cudaMemcpyDeviceToHost),
-              "reading a signal count");
-        collect(se);
-        const int64_t t_host = now_ns();
-        std::lock_guard<std::mutex> g(se.m);
-        const int64_t tm = st.t_mask.load(std::memory_order_acquire);
-        const int64_t td = st.t_done.load(std::memory_order_acquire);
-        se.lat_mask.push_back(1e-3 * static_cast<double>((tm ? tm : t_host) - p.t_submit));
-        se.lat_grouped.push_back(1e-3 * static_cast<double>((td ? td : t_host) - p.t_submit));
-        se.signal_counts[p.frame] = nsig;
-        se.frames_done++;
-        se.free_slots.push_back(p.slot);
-        se.cv.notify_all();
       }
-      Engine &e = *se.eng;
-      // finish() closes what is open; its spots are the last run's
-      for (Engine::Series &s : e.series)
-        s.lab->enqueue(0, e.plan->out(0), s.d_offs, e.plan->frame_count(0), s.d_map, s.d_caps,
-                       true, e.compute);
-      e.parity ^= 1;
-      e.synchronize();
-      collect(se);
     } catch (const std::exception &ex) {
       std::lock_guard<std::mutex> g(se.m);
       se.error = ex.what();
-      se.cv.notify_all();
     }
-    std::lock_guard<std::mutex> g(se.m);
+    std::unique_lock<std::mutex> lk(se.m);
+    se.worker_idle = true;
+    se.cv.notify_all();
+    se.cv.wait(lk, [&] { return se.inflight.empty(); });
+    lk.unlock();
+    try {
+      if (se.error.empty()) {
+        Engine &e = *se.eng;
+        // finish() closes what is open; its spots are read back directly
+        for (Engine::Series &s : e.series)
+          s.lab->enqueue(0, e.plan->out(0), s.d_offs, e.plan->frame_count(0), s.d_map,
+                         s.d_caps, true, e.compute);
+        e.parity ^= 1;
+        e.synchronize();
+        collect_direct(se);
+      }
+    } catch (const std::exception &ex) {
+      std::lock_guard<std::mutex> g(se.m);
+      se.error = ex.what();
+    }
+    lk.lock();
     se.done = true;
     se.cv.notify_all();
   }
 
-  // The spots the last run finished, appended with their latencies.
-  void collect(ServerSeries &se) {
+  // The runs' sinks, in frame order, as their host callbacks mark them. The
+  // sink of an in-flight slot is not reused until the slot is freed, so it
+  // is read without holding the series' lock.
+  void collect_loop(ServerSeries &se) {
+    while (true) {
+      Pending p;
+      {
+        std::unique_lock<std::mutex> lk(se.m);
+        se.cv.wait(lk, [&] { return !se.inflight.empty() || se.worker_idle; });
+        if (se.inflight.empty())
+          break;
+        p = se.inflight.front();
+      }
+      SlotState &st = *se.slot_state[p.slot];
+      {
+        std::unique_lock<std::mutex> dk(se.done_m);
+        se.done_cv.wait(dk, [&] { return st.t_done.load(std::memory_order_acquire) != 0; });
+      }
+      const SinkHeader h = *st.h_sink;
+      std::vector<Spot> sp;
+      std::vector<Pixel> px;
+      std::vector<double> lat;
+      if (!h.status) {
+        const Spot *hs = reinterpret_cast<const Spot *>(st.h_sink + 1);
+        const Pixel *hp = reinterpret_cast<const Pixel *>(hs + se.cap_spots);
+        sp.assign(hs, hs + h.nspots);
+        px.assign(hp, hp + h.npixels);
+      }
+      const int64_t t = now_ns();
+      std::lock_guard<std::mutex> g(se.m);
+      if (h.status && se.error.empty())
+        se.error = h.status & kSinkOverflow
+                       ? "frame " + std::to_string(p.frame) + " finished " +
+                             std::to_string(h.nspots) + " spots with " +
+                             std::to_string(h.npixels) + " pixels, more than its sink holds (" +
+                             std::to_string(se.cap_spots) + ", " + std::to_string(se.cap_pixels) +
+                             ")"
+                   : h.status & kSinkDecode ? "an uploaded chunk held a malformed LZ4 block"
+                   : h.status & kSinkLabel  ? "grouping capacity exceeded"
+                                            : "a threshold wait gave up";
+      if (!h.status) {
+        for (const Spot &s : sp) {
+          const int64_t last = static_cast<int64_t>(s.bbox[5]) - 1 - se.first_frame;
+          if (last >= 0 && last < static_cast<int64_t>(se.t_submit.size()))
+            se.lat_spot.push_back(1e-3 * static_cast<double>(t - se.t_submit[last]));
+        }
+        std::memcpy(&se.counts, h.counts, sizeof(se.counts));
+        if (!sp.empty())
+          se.spots.push_back(std::move(sp));
+        if (!px.empty())
+          se.pixels.push_back(std::move(px));
+      }
+      const int64_t tm = st.t_mask.load(std::memory_order_acquire);
+      const int64_t td = st.t_done.load(std::memory_order_acquire);
+      se.lat_mask.push_back(1e-3 * static_cast<double>((tm ? tm : td) - p.t_submit));
+      se.lat_grouped.push_back(1e-3 * static_cast<double>(td - p.t_submit));
+      se.signal_counts[p.frame] = h.nsig;
+      se.frames_done++;
+      se.inflight.pop_front();
+      se.free_slots.push_back(p.slot);
+      se.cv.notify_all();
+    }
+  }
+
+  // The spots the last enqueued work finished, read from the device.
+  void collect_direct(ServerSeries &se) {
     Engine &e = *se.eng;
     const LabelScalars &sc = e.group_state(0);
     const uint64_t ns = sc.batch_spots, np = sc.batch_pixels;
@@ -277,8 +441,10 @@ struct Server {
       if (last >= 0 && last < static_cast<int64_t>(se.t_submit.size()))
         se.lat_spot.push_back(1e-3 * static_cast<double>(t - se.t_submit[last]));
     }
-    se.spots.insert(se.spots.end(), sp.begin(), sp.end());
-    se.pixels.insert(se.pixels.end(), px.begin(), px.end());
+    if (!sp.empty())
+      se.spots.push_back(std::move(sp));
+    if (!px.empty())
+      se.pixels.push_back(std::move(px));
   }
 
   void stop(ServerSeries &se) {
@@ -289,6 +455,8 @@ struct Server {
     }
     if (se.worker.joinable())
       se.worker.join();
+    if (se.collector.joinable())
+      se.collector.join();
   }
 
   void close(int id) {
@@ -322,6 +490,21 @@ int copy_out(const std::vector<T> &v, T *out, size_t capacity, size_t *n) {
     return -2;
   if (!v.empty())
     std::memcpy(out, v.data(), v.size() * sizeof(T));
+  return 0;
+}
+
+template <typename T>
+int copy_blocks(const std::vector<std::vector<T>> &blocks, T *out, size_t capacity, size_t *n) {
+  size_t total = 0;
+  for (const auto &b : blocks)
+    total += b.size();
+  *n = total;
+  if (total > capacity)
+    return -2;
+  for (const auto &b : blocks) {
+    std::memcpy(out, b.data(), b.size() * sizeof(T));
+    out += b.size();
+  }
   return 0;
 }
 
@@ -412,7 +595,7 @@ int sf_server_spots(sf_server *server, int series, sf_spot *out, size_t capacity
       return -1;
     ServerSeries &se = reinterpret_cast<Server *>(server)->at(series);
     std::lock_guard<std::mutex> g(se.m);
-    return copy_out(se.spots, reinterpret_cast<sf::Spot *>(out), capacity, n);
+    return copy_blocks(se.spots, reinterpret_cast<sf::Spot *>(out), capacity, n);
   });
 }
 
@@ -422,7 +605,7 @@ int sf_server_pixels(sf_server *server, int series, sf_pixel *out, size_t capaci
       return -1;
     ServerSeries &se = reinterpret_cast<Server *>(server)->at(series);
     std::lock_guard<std::mutex> g(se.m);
-    return copy_out(se.pixels, reinterpret_cast<sf::Pixel *>(out), capacity, n);
+    return copy_blocks(se.pixels, reinterpret_cast<sf::Pixel *>(out), capacity, n);
   });
 }
 

@@ -54,6 +54,9 @@ public:
                size_t width, void *dst, size_t dst_pitch, cudaStream_t s);
   // Whether a block failed since the last call (synchronises the device).
   bool take_error();
+  // The device flag itself (nonzero after a failed block), allocated and
+  // cleared on first use.
+  int *error_flag();
 
 private:
   uint8_t *d_chunk_ = nullptr;

@@ -54,6 +54,10 @@ struct Engine {
   // slot's argument. Set them before the first run.
   cudaHostFn_t on_mask = nullptr, on_done = nullptr;
   std::vector<void *> hook_args;
+  // Enqueued after the grouping and before on_done, for work that must see
+  // the run's results before the next run overwrites them.
+  void (*post_run)(Engine &engine, int slot, void *arg) = nullptr;
+  void *post_arg = nullptr;
 
   ~Engine() {
     if (compute)
@@ -108,6 +112,8 @@ struct Engine {
     for (Series &se : series)
       se.lab->enqueue(se.nframes, plan->out(slot), se.d_offs, plan->frame_count(slot), se.d_map,
                       se.d_caps, false, compute);
+    if (post_run)
+      post_run(*this, slot, post_arg);
     if (on_done)
       check(cudaLaunchHostFunc(compute, on_done, hook_args[slot]), "cudaLaunchHostFunc");
   }
