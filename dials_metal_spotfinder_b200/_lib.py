@@ -95,6 +95,7 @@ SIGNATURES = {
     "sf_server_create": (_I, [_P, ctypes.POINTER(_P)]),
     "sf_server_destroy": (None, [_P]),
     "sf_server_open": (_I, [_P, _S, _S, _I, _P, ctypes.c_int64, ctypes.POINTER(_I)]),
+    "sf_server_set_pixel_mask": (_I, [_P, _I, _P]),
     "sf_server_submit": (_I, [_P, _I, _P, _S, _I, ctypes.c_int64]),
     "sf_server_close": (_I, [_P, _I]),
     "sf_server_stats": (_I, [_P, _I, _P, _P]),
@@ -108,6 +109,7 @@ SIGNATURES = {
     "sf_engine_upload": (_I, [_P, _I, _I, _P]),
     "sf_engine_upload_device": (_I, [_P, _I, _I, _P, _S]),
     "sf_engine_upload_chunk": (_I, [_P, _I, _I, _P, _S, _I]),
+    "sf_engine_set_pixel_mask": (_I, [_P, _I, _P]),
     "sf_engine_run": (_I, [_P, _I]),
     "sf_engine_use_graph": (_I, [_P, _I]),
     "sf_engine_synchronize": (_I, [_P]),

@@ -124,6 +124,15 @@ int sf_engine_upload_chunk(sf_engine *engine, int slot, int frame, const void *c
   });
 }
 
+int sf_engine_set_pixel_mask(sf_engine *engine, int frame, const uint8_t *mask) {
+  return guarded([&] {
+    if (!engine)
+      return -1;
+    reinterpret_cast<Engine *>(engine)->set_pixel_mask(frame, mask);
+    return 0;
+  });
+}
+
 int sf_engine_run(sf_engine *engine, int slot) {
   return guarded([&] {
     if (!engine)

@@ -552,6 +552,19 @@ int sf_server_open(sf_server *server, size_t height, size_t width, int elem_byte
   });
 }
 
+int sf_server_set_pixel_mask(sf_server *server, int series, const uint8_t *mask) {
+  return guarded([&] {
+    if (!server)
+      return -1;
+    ServerSeries &se = reinterpret_cast<Server *>(server)->at(series);
+    std::lock_guard<std::mutex> g(se.m);
+    if (se.frames_done || !se.queue.empty() || !se.inflight.empty() || !se.eng)
+      throw std::invalid_argument("set a series' pixel mask before its first frame");
+    se.eng->set_pixel_mask(0, mask);
+    return 0;
+  });
+}
+
 int sf_server_submit(sf_server *server, int series, const void *chunk, size_t nbytes,
                      int algorithm, int64_t timeout_us) {
   return guarded([&] {

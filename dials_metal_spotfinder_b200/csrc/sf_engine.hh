@@ -58,6 +58,11 @@ struct Engine {
   // the run's results before the next run overwrites them.
   void (*post_run)(Engine &engine, int slot, void *arg) = nullptr;
   void *post_arg = nullptr;
+  // The pixel mask: per frame, the masked pixels' element offsets from frame
+  // 0's origin (the same in every slot), and all of them on the device.
+  std::vector<std::vector<uint64_t>> mask_offsets;
+  uint64_t *d_mask = nullptr;
+  uint64_t mask_n = 0;
 
   ~Engine() {
     if (compute)
@@ -67,6 +72,7 @@ struct Engine {
     for (cudaGraphExec_t g : graphs)
       if (g)
         cudaGraphExecDestroy(g);
+    cudaFree(d_mask);
     for (Series &se : series) {
       se.lab.reset();
       cudaFree(se.d_offs);
@@ -104,6 +110,10 @@ struct Engine {
 
   // Threshold, placement and (when enabled) grouping of one slot.
   void enqueue_body(int slot, cudaEvent_t b, cudaEvent_t c) {
+    if (mask_n)
+      check(launch_stamp_mask(plan->frame_origin(slot, 0), plan->elem_bytes(), d_mask, mask_n,
+                              compute),
+            "launching the mask stamp");
     plan->enqueue(slot, compute, b);
     if (c)
       check(cudaEventRecord(c, compute), "cudaEventRecord");
@@ -255,6 +265,47 @@ struct Engine {
     check(cudaStreamWaitEvent(copy, consumed[slot], 0), "ordering after the last run");
     plan->upload_device(slot, frame, dev, pitch, copy);
     check(cudaEventRecord(uploaded[slot], copy), "cudaEventRecord");
+  }
+
+  // Frame `frame`'s pixel mask (height x width bytes, nonzero = masked), or
+  // none with a null mask. Waits for the device; captured graphs are dropped
+  // so the next runs stamp the new mask.
+  void set_pixel_mask(int frame, const uint8_t *mask) {
+    check_frame(frame);
+    const ThresholdPlan::Shape &sh = plan->shape(frame);
+    const uint64_t eb = static_cast<uint64_t>(plan->elem_bytes());
+    const uint64_t at = (static_cast<uint64_t>(
+                             static_cast<const char *>(plan->frame_origin(0, frame)) -
+                             static_cast<const char *>(plan->frame_origin(0, 0)))) /
+                        eb;
+    if (mask_offsets.size() < static_cast<size_t>(plan->nframes()))
+      mask_offsets.resize(plan->nframes());
+    std::vector<uint64_t> &v = mask_offsets[frame];
+    v.clear();
+    if (mask)
+      for (int64_t y = 0; y < sh.height; y++)
+        for (int64_t x = 0; x < sh.width; x++)
+          if (mask[y * sh.width + x])
+            v.push_back(at + static_cast<uint64_t>(y) * plan->pitch() + x);
+    std::vector<uint64_t> all;
+    for (const auto &f : mask_offsets)
+      all.insert(all.end(), f.begin(), f.end());
+    check(cudaStreamSynchronize(copy), "cudaStreamSynchronize");
+    check(cudaStreamSynchronize(compute), "cudaStreamSynchronize");
+    cudaFree(d_mask);
+    d_mask = nullptr;
+    mask_n = 0;
+    if (!all.empty()) {
+      check(cudaMalloc(&d_mask, all.size() * sizeof(uint64_t)), "cudaMalloc pixel mask");
+      check(cudaMemcpy(d_mask, all.data(), all.size() * sizeof(uint64_t), cudaMemcpyHostToDevice),
+            "copying the pixel mask");
+      mask_n = all.size();
+    }
+    for (cudaGraphExec_t &g : graphs)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
   }
 
   void upload_chunk(int slot, int frame, const void *chunk, size_t nbytes, int algorithm) {

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -68,6 +69,10 @@ constexpr int kPlaceItems = 4;
 constexpr int kPlaceTiles = kPlaceThreads * kPlaceItems;
 
 cudaError_t launch_place(const PlaceLaunch &L, cudaStream_t stream);
+
+// Writes the type's maximum at base[offsets[i]], i < n (mask.cu).
+cudaError_t launch_stamp_mask(void *base, int elem_bytes, const uint64_t *offsets, uint64_t n,
+                              cudaStream_t s);
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point, so the
 // library needs no link against libcuda.

@@ -78,6 +78,17 @@ class Engine:
         raise_for(lib.sf_engine_upload_chunk(self._h, slot, frame, chunk.ctypes.data, len(chunk),
                                              algorithm_code(algorithm)), "upload_chunk")
 
+    def set_pixel_mask(self, frame: int, mask) -> None:
+        """Frame `frame`'s pixel mask (nonzero = masked), stamped as the masked
+        sentinel before every threshold; None clears it."""
+        if mask is None:
+            raise_for(lib.sf_engine_set_pixel_mask(self._h, frame, None), "set_pixel_mask")
+            return
+        mask = np.ascontiguousarray(mask != 0, dtype=np.uint8)
+        if mask.shape != self.shapes[frame]:
+            raise ValueError("mask shape does not match the frame")
+        raise_for(lib.sf_engine_set_pixel_mask(self._h, frame, mask.ctypes.data), "set_pixel_mask")
+
     def run(self, slot: int = 0) -> None:
         raise_for(lib.sf_engine_run(self._h, slot), "run")
 

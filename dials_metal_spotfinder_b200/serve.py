@@ -57,6 +57,12 @@ class Server:
         raise_for(status, "sf_server_open")
         return sid.value
 
+    def set_pixel_mask(self, series: int, mask: np.ndarray) -> None:
+        """Before the series' first frame: nonzero = masked."""
+        mask = np.ascontiguousarray(mask != 0, dtype=np.uint8)
+        raise_for(lib.sf_server_set_pixel_mask(self._h, series, mask.ctypes.data),
+                  "sf_server_set_pixel_mask")
+
     def submit(self, series: int, chunk: np.ndarray, algorithm="bslz4", timeout_s=1.0) -> bool:
         """False if no slot freed up within the timeout (the frame is dropped)."""
         status = lib.sf_server_submit(self._h, series, chunk.ctypes.data, len(chunk),

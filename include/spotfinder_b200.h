@@ -251,6 +251,13 @@ SF_API int sf_engine_upload_device(sf_engine *engine, int slot, int frame,
  * unchanged until the next synchronize. */
 SF_API int sf_engine_upload_chunk(sf_engine *engine, int slot, int frame, const void *chunk,
                                   size_t nbytes, int algorithm);
+/* The detector's pixel mask for frame `frame` (height x width bytes,
+ * nonzero = a pixel not to use, as NXmx /entry/instrument/detector/
+ * pixel_mask marks them), stamped into the frame as the masked sentinel
+ * before every run's threshold; NULL clears it. No reference counterpart:
+ * the reference reads no pixel mask (its one documented omission) and relies
+ * on the sentinels in the data. Waits for the device. */
+SF_API int sf_engine_set_pixel_mask(sf_engine *engine, int frame, const uint8_t *mask);
 /* Enqueue the threshold of every frame of a slot, after its uploads. */
 SF_API int sf_engine_run(sf_engine *engine, int slot);
 /* Replay each slot's run from a CUDA graph captured on first use. */
@@ -333,6 +340,9 @@ SF_API void sf_server_destroy(sf_server *server);
  * does not fit in what is left of the budget (retry after a close). */
 SF_API int sf_server_open(sf_server *server, size_t height, size_t width, int elem_bytes,
                           const sf_group_options *options, int64_t first_frame, int *series);
+/* The series' pixel mask (height x width bytes, nonzero = masked), as
+ * sf_engine_set_pixel_mask; before the series' first frame. */
+SF_API int sf_server_set_pixel_mask(sf_server *server, int series, const uint8_t *mask);
 /* The series' next frame, as a chunk (SF_CHUNK_*), copied before return.
  * Waits up to timeout_us for a free slot; -2 if none freed: the frame is
  * dropped (its number is skipped, which closes the open components, as a

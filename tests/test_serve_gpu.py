@@ -111,3 +111,24 @@ def test_latency_report(gpu_lib):
     for key in ("frame_to_mask_ms", "frame_to_grouped_ms", "frame_to_spot_ms"):
         assert 0 < r[key]["p50"] <= r[key]["p99"] <= r[key]["max"]
     assert r["frame_to_mask_ms"]["p50"] <= r["frame_to_grouped_ms"]["p50"]
+
+
+def test_pixel_mask_in_a_served_series(gpu_lib):
+    from dials_metal_spotfinder_b200.serve import Server
+    s, frames, two_d = series_a()
+    mask = np.zeros(frames[0].shape, bool)
+    mask[100:130, 200:260] = True
+    mask[:, 17] = True
+    with Server() as srv:
+        sid = srv.open(frames[0].shape, two_d=two_d)
+        srv.set_pixel_mask(sid, mask)
+        for c in encode_all(frames):
+            assert srv.submit(sid, c, timeout_s=30)
+        srv.finish(sid)
+        got = results(srv, sid)
+    stamped = []
+    for f in frames:
+        f = f.copy()
+        f[mask] = 0xFFFF
+        stamped.append(f)
+    check_oracle(stamped, two_d, *got)
