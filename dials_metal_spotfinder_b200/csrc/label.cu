@@ -69,6 +69,7 @@ struct LabArgs {
   uint32_t *bits, *bcnt;
   uint32_t *comp_root, *msize, *members;
   uint64_t *mpk;
+  uint32_t *runs; // per batch: 2 g for a run's first pixel, 2 g + 1 for a chunk-crossing link
   Spot *spot_tmp;
   Pixel *pix_tmp;
   uint64_t *pack;
@@ -201,6 +202,7 @@ __global__ void lab_setup(LabArgs a) {
   sc->seg_len = static_cast<uint64_t>(nseg) * sc->nw;
   sc->signal_pixels += pos - carry;
   sc->closed32 = sc->open32 = 0;
+  sc->runs_n = 0;
   sc->members_pack = 0;
   sc->accepted_pack = 0;
 }
@@ -222,14 +224,18 @@ __device__ __forceinline__ const uint32_t *table_of(const LabArgs &a, int s, int
 // start one level deep; a run that enters a chunk from the previous one is
 // joined by lab_link at the chunk's first position.
 __global__ void __launch_bounds__(kThreads) lab_gather(LabArgs a) {
-  const LabelScalars *sc = a.sc;
+  LabelScalars *sc = a.sc;
   const uint64_t n = sc->n, carry = sc->carry_n;
   const int nseg = static_cast<int>(sc->nseg);
   const int first_batch_seg = carry > 0 ? 1 : 0;
   const uint32_t W = static_cast<uint32_t>(a.width);
-  const int lane = threadIdx.x & 31;
-  const uint64_t warps = gstride() >> 5;
-  for (uint64_t base = (gtid() >> 5) * 32; base < n; base += warps * 32) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __shared__ uint32_t warp_count[kThreads / 32];
+  __shared__ uint32_t block_at;
+  // block-uniform trip count: the run list is appended to once per block
+  for (uint64_t block_base = static_cast<uint64_t>(blockIdx.x) * kThreads; block_base < n;
+       block_base += static_cast<uint64_t>(gridDim.x) * kThreads) {
+    const uint64_t base = block_base + static_cast<uint64_t>(warp) * 32;
     const uint64_t g = base + lane;
     bool left = false;
     if (g < n) {
@@ -258,13 +264,36 @@ __global__ void __launch_bounds__(kThreads) lab_gather(LabArgs a) {
       }
     }
     const uint32_t linked = __ballot_sync(kFull, left);
-    if (g < n && g >= carry) {
+    const bool mine = g < n && g >= carry;
+    if (mine) {
       // the run's first lane in this chunk: the highest lane at or below
       // this one that is not joined to its left neighbour
       const uint32_t starts = ~linked & (0xffffffffu >> (31 - lane));
       const int first = starts ? 31 - __clz(starts) : 0;
       a.par[g] = static_cast<uint32_t>(base + first);
     }
+    // lab_link's work list: every run's first pixel, and the first lane of
+    // a chunk that a run enters from the chunk before
+    const bool boundary = left && lane == 0;
+    const bool entry = mine && (!left || boundary);
+    const uint32_t want = __ballot_sync(kFull, entry);
+    if (lane == 0)
+      warp_count[warp] = __popc(want);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t total = 0;
+      for (int w = 0; w < kThreads / 32; w++) {
+        const uint32_t c = warp_count[w];
+        warp_count[w] = total;
+        total += c;
+      }
+      block_at = total ? atomicAdd(&sc->runs_n, total) : 0u;
+    }
+    __syncthreads();
+    if (entry)
+      a.runs[block_at + warp_count[warp] + __popc(want & ((1u << lane) - 1u))] =
+          (static_cast<uint32_t>(g) << 1) | (boundary ? 1u : 0u);
+    __syncthreads();
   }
 }
 
@@ -310,17 +339,23 @@ __global__ void __launch_bounds__(kThreads) lab_link(LabArgs a) {
   const int first_batch_seg = carry > 0 ? 1 : 0;
   const uint32_t W = static_cast<uint32_t>(a.width);
   const int64_t z0 = sc->batch_z0;
-  for (uint64_t g = carry + gtid(); g < n; g += gstride()) {
+  const uint32_t nruns = sc->runs_n;
+  (void)n;
+  (void)carry;
+  // one entry of lab_gather's list per thread, so the lanes of a warp all
+  // have a run to link
+  for (uint64_t i = gtid(); i < nruns; i += gstride()) {
+    const uint32_t e = a.runs[i];
+    const uint64_t g = e >> 1;
+    if (e & 1u) { // a run crossing into a new chunk
+      uf_unite(a.par, static_cast<uint32_t>(g), static_cast<uint32_t>(g - 1));
+      continue;
+    }
     // the batch's frames are consecutive: a new pixel's frame is its segment
     const int s = first_batch_seg + static_cast<int>(a.fr[g] - z0);
     const uint64_t s0 = a.seg_start[s];
     const uint64_t end = s0 + a.seg_count[s];
     const uint32_t idx = a.ix[g];
-    if (g > s0 && idx % W != 0 && a.ix[g - 1] + 1 == idx) {
-      if ((g & 31) == 0)
-        uf_unite(a.par, static_cast<uint32_t>(g), static_cast<uint32_t>(g - 1));
-      continue;
-    }
     uint32_t last = idx; // the run's last index
     for (uint64_t e = g + 1; e < end; e++) {
       const uint32_t v = a.ix[e];
@@ -1077,7 +1112,7 @@ void DeviceLabeller::release() {
     l = Live();
   }
   void *ptrs[] = {root_, size_, rank_of_root_, cursor_, lastz_, bits_, bcnt_, comp_root_,
-                  msize_, mpk_, spot_tmp_, pix_tmp_, members_, pack_, open_, spots_out_, kept_out_, seg_start_,
+                  msize_, mpk_, runs_, spot_tmp_, pix_tmp_, members_, pack_, open_, spots_out_, kept_out_, seg_start_,
                   seg_count_, seg_z_, tab_};
   for (void *p : ptrs)
     cudaFree(p);
@@ -1086,6 +1121,7 @@ void DeviceLabeller::release() {
   lastz_ = nullptr;
   bits_ = bcnt_ = comp_root_ = msize_ = members_ = open_ = nullptr;
   mpk_ = pack_ = nullptr;
+  runs_ = nullptr;
   spot_tmp_ = nullptr;
   pix_tmp_ = nullptr;
   spots_out_ = nullptr;
@@ -1101,7 +1137,7 @@ void DeviceLabeller::reserve(uint64_t batch_pixels, int max_frames, uint64_t car
   const int fc = std::max(max_frames, frame_cap_);
   const uint64_t cc = std::max(carry_pixels, carry_cap_);
   const uint64_t live = bc + cc;
-  if (live >= 0xffffffffull)
+  if (live >= 0x7fffffffull)
     throw std::invalid_argument("labelling batch too large");
   // Growing keeps the carry: copy it across after reallocating.
   check(cudaDeviceSynchronize(), "cudaDeviceSynchronize");
@@ -1140,6 +1176,7 @@ void DeviceLabeller::reserve(uint64_t batch_pixels, int max_frames, uint64_t car
     alloc(&comp_root_, live, "components");
     alloc(&msize_, live, "member sizes");
     alloc(&mpk_, live, "member offsets");
+    alloc(&runs_, live, "run list");
     alloc(&members_, live, "members");
     alloc(&pack_, live, "spot offsets");
     alloc(&open_, live, "open flags");
@@ -1224,6 +1261,7 @@ void DeviceLabeller::enqueue(int nframes, const SignalPixel *lists, const uint64
   a.comp_root = comp_root_;
   a.msize = msize_;
   a.mpk = mpk_;
+  a.runs = runs_;
   a.spot_tmp = spot_tmp_;
   a.pix_tmp = pix_tmp_;
   a.members = members_;

@@ -50,6 +50,7 @@ struct LabelScalars {
   uint64_t seg_len;       // nseg * nw
   uint64_t closed;        // finished components
   uint32_t closed32, open32;
+  uint32_t runs_n, pad0;  // lab_link's work list
   uint64_t members_pack;  // members (low 32) | components passing the size filters (high 32)
   uint64_t accepted_pack; // accepted spots (low 32) | their pixels (high 32)
   uint64_t batch_spots, batch_pixels;
@@ -130,6 +131,7 @@ private:
   uint32_t *bits_ = nullptr, *bcnt_ = nullptr; // bucket bitmaps and their word counts
   uint32_t *comp_root_ = nullptr, *msize_ = nullptr, *members_ = nullptr;
   uint64_t *mpk_ = nullptr; // member offset (low 32) | size-filtered index (high 32)
+  uint32_t *runs_ = nullptr; // lab_link's work list
   Spot *spot_tmp_ = nullptr;  // spots by size-filtered index, before acceptance
   Pixel *pix_tmp_ = nullptr;  // their pixels, by member offset
   uint64_t *pack_ = nullptr;
