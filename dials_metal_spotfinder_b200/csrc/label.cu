@@ -634,15 +634,28 @@ constexpr uint32_t kCompCap = 1024;
 struct WarpBuffers {
   uint32_t *g, *ix, *val;
   int32_t *fr;
+  double *t; // 3 x 32 second-pass terms
 };
 
+// Per warp: four CAP-member arrays and the terms. Two launches split the
+// components by size: up to kSmallCap members with small buffers, so that
+// many warps fit on an SM, and the rest with kCompCap-member buffers.
+constexpr uint32_t kSmallCap = 512;
+
+template <uint32_t CAP> __host__ __device__ constexpr size_t warp_comp_bytes() {
+  return 4 * CAP * sizeof(uint32_t) + 3 * 32 * sizeof(double);
+}
+
+template <uint32_t CAP>
 __device__ __forceinline__ WarpBuffers warp_buffers(unsigned char *smem, int warp) {
   WarpBuffers b;
-  uint32_t *base = reinterpret_cast<uint32_t *>(smem) + static_cast<size_t>(warp) * 4 * kCompCap;
+  unsigned char *at = smem + static_cast<size_t>(warp) * warp_comp_bytes<CAP>();
+  uint32_t *base = reinterpret_cast<uint32_t *>(at);
   b.g = base;
-  b.ix = base + kCompCap;
-  b.val = base + 2 * kCompCap;
-  b.fr = reinterpret_cast<int32_t *>(base + 3 * kCompCap);
+  b.ix = base + CAP;
+  b.val = base + 2 * CAP;
+  b.fr = reinterpret_cast<int32_t *>(base + 3 * CAP);
+  b.t = reinterpret_cast<double *>(base + 4 * CAP);
   return b;
 }
 
@@ -871,27 +884,33 @@ __device__ bool spot_pass_warp(uint32_t W, double max_sep, const WarpBuffers &b,
   if (sum > 0.0) {
     const double mx = __ddiv_rn(wx, sum), my = __ddiv_rn(wy, sum);
     double mz = __ddiv_rn(wz, sum);
-    double dx2 = 0.0, dy2 = 0.0, dz2 = 0.0;
+    // lanes 0, 1 and 2 each run one of the three sums, over terms the
+    // whole warp computes 32 at a time
+    double acc = 0.0;
     for (uint32_t c = 0; c < n; c += 32) {
       const uint32_t k = c + lane;
-      double tx = 0.0, ty = 0.0, tz = 0.0;
       if (k < n) {
         const uint32_t idx = b.ix[k];
         const double value = __uint2double_rn(b.val[k]);
         const double dx = __dsub_rn(__dadd_rn(__uint2double_rn(idx % W), 0.5), mx);
         const double dy = __dsub_rn(__dadd_rn(__uint2double_rn(idx / W), 0.5), my);
         const double dz = __dsub_rn(__dadd_rn(__int2double_rn(b.fr[k]), 0.5), mz);
-        tx = __dmul_rn(__dmul_rn(value, dx), dx);
-        ty = __dmul_rn(__dmul_rn(value, dy), dy);
-        tz = __dmul_rn(__dmul_rn(value, dz), dz);
+        b.t[lane] = __dmul_rn(__dmul_rn(value, dx), dx);
+        b.t[32 + lane] = __dmul_rn(__dmul_rn(value, dy), dy);
+        b.t[64 + lane] = __dmul_rn(__dmul_rn(value, dz), dz);
       }
-      const uint32_t cnt = min(32u, n - c);
-      for (uint32_t j = 0; j < cnt; j++) {
-        dx2 = __dadd_rn(dx2, __shfl_sync(kFull, tx, j));
-        dy2 = __dadd_rn(dy2, __shfl_sync(kFull, ty, j));
-        dz2 = __dadd_rn(dz2, __shfl_sync(kFull, tz, j));
+      __syncwarp();
+      if (lane < 3) {
+        const uint32_t cnt = min(32u, n - c);
+        const double *t = b.t + 32 * lane;
+        for (uint32_t j = 0; j < cnt; j++)
+          acc = __dadd_rn(acc, t[j]);
       }
+      __syncwarp();
     }
+    const double dx2 = __shfl_sync(kFull, acc, 0);
+    const double dy2 = __shfl_sync(kFull, acc, 1);
+    const double dz2 = __shfl_sync(kFull, acc, 2);
     const double ss = __dmul_rn(sum, sum);
     if (ss > sum_sq) {
       const double den = __dsub_rn(ss, sum_sq);
@@ -929,28 +948,34 @@ __device__ bool spot_pass_warp(uint32_t W, double max_sep, const WarpBuffers &b,
 // run the spot pass, and park the spot and its pixel records by the
 // component's size-filtered index and member offset until lab_write knows
 // where the accepted ones go.
-__global__ void __launch_bounds__(kCompWarps * 32) lab_accept(LabArgs a) {
+// Components of lo < size <= hi; the launch with lo = 0 also clears the
+// pack word of those the size filter removed.
+template <uint32_t CAP>
+__global__ void __launch_bounds__(kCompWarps * 32) lab_accept(LabArgs a, uint32_t lo,
+                                                              uint32_t hi) {
   extern __shared__ __align__(16) unsigned char comp_smem[];
   LabelScalars *sc = a.sc;
   const uint64_t closed = sc->closed;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const WarpBuffers b = warp_buffers(comp_smem, warp);
+  const WarpBuffers b = warp_buffers<CAP>(comp_smem, warp);
   const uint32_t W = static_cast<uint32_t>(a.width);
   uint32_t separated = 0;
   const uint64_t gw = gtid() >> 5, nw = gstride() >> 5;
   for (uint64_t r = gw; r < closed; r += nw) {
     const uint32_t n = a.msize[r];
     if (n == 0) {
-      if (lane == 0)
+      if (lane == 0 && lo == 0)
         a.pack[r] = 0;
       continue;
     }
+    if (n <= lo || n > hi)
+      continue;
     const uint32_t moff = static_cast<uint32_t>(a.mpk[r]);
     const uint32_t sidx = static_cast<uint32_t>(a.mpk[r] >> 32);
     uint32_t *m = a.members + moff;
     Spot spot{}; // zeroed, padding included, so rows compare byte for byte
     bool ok;
-    if (n <= kCompCap) {
+    if (n <= CAP) {
       load_members(a, m, n, true, b, lane);
       if (!spot_pass_warp(W, a.max_sep, b, n, lane, &spot, &ok))
         ok = spot_pass(W, a.max_sep, SharedMembers{b.ix, b.val, b.fr}, n, &spot);
@@ -1025,7 +1050,6 @@ __global__ void __launch_bounds__(kThreads) lab_write(LabArgs a) {
   }
 }
 
-constexpr size_t kCompSmem = static_cast<size_t>(kCompWarps) * 4 * kCompCap * sizeof(uint32_t);
 
 __global__ void __launch_bounds__(kThreads) lab_open(LabArgs a) {
   const uint64_t n = a.sc->n;
@@ -1087,15 +1111,26 @@ DeviceLabeller::DeviceLabeller(int height, int width, const GroupOptions &option
   check(cudaMemset(sc_, 0, sizeof(LabelScalars)), "clearing labeller scalars");
   nblk_ = ((static_cast<uint64_t>(height) * width) >> kBlockShift) + 2;
   check(cudaMalloc(&carry_tab_, nblk_ * sizeof(uint32_t)), "cudaMalloc carry table");
-  check(cudaFuncSetAttribute(lab_accept, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(kCompSmem)),
+  check(cudaFuncSetAttribute(lab_accept<kCompCap>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(kCompWarps * warp_comp_bytes<kCompCap>())),
         "cudaFuncSetAttribute");
   grid_ = static_cast<unsigned>(device_sm_count() * 8);
   check(cudaMallocHost(&z_stage_, sizeof(int64_t)), "cudaMallocHost");
+  check(cudaStreamCreateWithFlags(&aux_, cudaStreamNonBlocking), "cudaStreamCreate");
+  check(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "cudaEventCreate");
+  check(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming), "cudaEventCreate");
   check(cudaStreamSynchronize(cudaStreamLegacy), "clearing labeller scalars");
 }
 
 DeviceLabeller::~DeviceLabeller() {
+  if (aux_) {
+    cudaStreamSynchronize(aux_);
+    cudaStreamDestroy(aux_);
+  }
+  if (fork_)
+    cudaEventDestroy(fork_);
+  if (join_)
+    cudaEventDestroy(join_);
   release();
   cudaFree(sc_);
   cudaFree(carry_tab_);
@@ -1294,7 +1329,15 @@ void DeviceLabeller::enqueue(int nframes, const SignalPixel *lists, const uint64
   lab_rank<<<grid, kThreads, 0, s>>>(a);
   scan64_.run(mpk_, mpk_, &sc->closed, 1, live_cap_, &sc->members_pack, s);
   lab_scatter<<<grid, kThreads, 0, s>>>(a);
-  lab_accept<<<grid, kCompWarps * 32, kCompSmem, s>>>(a);
+  // the few large components on a second stream, beside the many small
+  check(cudaEventRecord(fork_, s), "cudaEventRecord");
+  check(cudaStreamWaitEvent(aux_, fork_, 0), "cudaStreamWaitEvent");
+  lab_accept<kCompCap><<<grid_ / 4, kCompWarps * 32, kCompWarps * warp_comp_bytes<kCompCap>(),
+                         aux_>>>(a, kSmallCap, 0xffffffffu);
+  lab_accept<kSmallCap><<<grid, kCompWarps * 32, kCompWarps * warp_comp_bytes<kSmallCap>(), s>>>(
+      a, 0u, kSmallCap);
+  check(cudaEventRecord(join_, aux_), "cudaEventRecord");
+  check(cudaStreamWaitEvent(s, join_, 0), "cudaStreamWaitEvent");
   scan64_.run(pack_, pack_, &sc->closed, 1, live_cap_, &sc->accepted_pack, s);
   lab_write<<<grid, kThreads, 0, s>>>(a);
   lab_open<<<grid, kThreads, 0, s>>>(a);
