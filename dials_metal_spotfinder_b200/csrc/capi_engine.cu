@@ -24,6 +24,8 @@ std::unique_ptr<Engine> make_engine(int elem_bytes, const std::vector<ThresholdP
   auto e = std::make_unique<Engine>();
   check(cudaStreamCreateWithFlags(&e->compute, cudaStreamNonBlocking), "stream");
   check(cudaStreamCreateWithFlags(&e->copy, cudaStreamNonBlocking), "stream");
+  check(cudaStreamCreateWithFlags(&e->group, cudaStreamNonBlocking), "stream");
+  check(cudaEventCreateWithFlags(&e->join, cudaEventDisableTiming), "event");
   e->plan = std::make_unique<ThresholdPlan>(elem_bytes, shapes, tuning, slots);
   for (int s = 0; s < slots; s++) {
     cudaEvent_t u, c;
@@ -33,7 +35,15 @@ std::unique_ptr<Engine> make_engine(int elem_bytes, const std::vector<ThresholdP
     e->consumed.push_back(c);
     check(cudaEventRecord(u, e->copy), "event");
     check(cudaEventRecord(c, e->compute), "event");
+    cudaEvent_t p, g;
+    check(cudaEventCreateWithFlags(&p, cudaEventDisableTiming), "event");
+    e->placed.push_back(p);
+    check(cudaEventCreateWithFlags(&g, cudaEventDisableTiming), "event");
+    e->grouped.push_back(g);
+    check(cudaEventRecord(p, e->compute), "event");
+    check(cudaEventRecord(g, e->group), "event");
   }
+  e->thr_graphs.assign(slots, nullptr);
   e->graphs.assign(2 * slots, nullptr);
   e->hook_args.assign(slots, nullptr);
   for (cudaEvent_t &m : e->marks)
@@ -213,7 +223,7 @@ int sf_engine_record(sf_engine *engine, int mark) {
     if (!engine || mark < 0 || mark >= sf::kMarks)
       return -1;
     Engine *e = reinterpret_cast<Engine *>(engine);
-    sf::check(cudaEventRecord(e->marks[mark], e->compute), "cudaEventRecord");
+    e->record(e->marks[mark]);
     return 0;
   });
 }
@@ -381,7 +391,7 @@ int sf_engine_finish(sf_engine *engine) {
       throw std::invalid_argument("grouping is not enabled");
     for (Engine::Series &se : e->series)
       se.lab->enqueue(0, e->plan->out(0), se.d_offs, e->plan->frame_count(0), se.d_map,
-                      se.d_caps, true, e->compute);
+                      se.d_caps, true, e->group);
     e->parity ^= 1;
     return 0;
   });

@@ -165,7 +165,7 @@ void CUDART_CB mark_done(void *arg) {
 void post_run_sink(Engine &e, int slot, void *arg) {
   ServerSeries *se = static_cast<ServerSeries *>(arg);
   DeviceLabeller &lab = *e.series[0].lab;
-  sink_results<<<64, 256, 0, e.compute>>>(lab.scalars(), lab.batch_spots(), lab.batch_pixels(),
+  sink_results<<<64, 256, 0, e.group>>>(lab.scalars(), lab.batch_spots(), lab.batch_pixels(),
                                           e.plan->frame_count(slot), e.plan->status(slot),
                                           e.decoder.error_flag(),
                                           se->slot_state[slot]->d_sink, se->cap_spots,
@@ -308,7 +308,7 @@ struct Server {
         if (p.frame != expected) {
           // frames were dropped: the gap closes everything open, as a gap
           // in the numbering does for the reference's Labeller
-          e.series[0].lab->set_next_frame(se.first_frame + p.frame, e.compute);
+          e.series[0].lab->set_next_frame(se.first_frame + p.frame, e.group);
           expected = p.frame;
         }
         SlotState &st = *se.slot_state[p.slot];
@@ -338,7 +338,7 @@ struct Server {
         // finish() closes what is open; its spots are read back directly
         for (Engine::Series &s : e.series)
           s.lab->enqueue(0, e.plan->out(0), s.d_offs, e.plan->frame_count(0), s.d_map,
-                         s.d_caps, true, e.compute);
+                         s.d_caps, true, e.group);
         e.parity ^= 1;
         e.synchronize();
         collect_direct(se);

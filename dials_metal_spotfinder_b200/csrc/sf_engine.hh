@@ -20,10 +20,20 @@ constexpr int kRunEvents = 4;
 
 struct Engine {
   std::unique_ptr<ThresholdPlan> plan;
-  cudaStream_t compute = nullptr, copy = nullptr;
-  std::vector<cudaEvent_t> uploaded, consumed; // per slot
-  // Graphs per (slot, labeller parity): the labeller alternates between two
-  // live buffers, so a captured run is only valid for the parity it saw.
+  // Streams: uploads on `copy`; threshold and placement on `compute`; the
+  // grouping, when enabled, on `group`, so that the next run's threshold
+  // overlaps this run's grouping. Per slot, events order the upload before
+  // the threshold (uploaded), the threshold before the next upload
+  // (consumed), the placement before the grouping (placed) and the grouping
+  // before the slot's lists are overwritten (grouped).
+  cudaStream_t compute = nullptr, copy = nullptr, group = nullptr;
+  std::vector<cudaEvent_t> uploaded, consumed, placed, grouped;
+  cudaEvent_t join = nullptr; // the compute stream's work, for the group stream
+  int last_slot = -1;
+  // Graphs: per slot, the threshold and placement; per (slot, labeller
+  // parity), the grouping -- the labeller alternates between two live
+  // buffers, so a captured grouping is only valid for the parity it saw.
+  std::vector<cudaGraphExec_t> thr_graphs;
   std::vector<cudaGraphExec_t> graphs;
   bool use_graph = false;
   cudaEvent_t marks[kMarks] = {};
@@ -69,9 +79,9 @@ struct Engine {
       cudaStreamSynchronize(compute);
     if (copy)
       cudaStreamSynchronize(copy);
-    for (cudaGraphExec_t g : graphs)
-      if (g)
-        cudaGraphExecDestroy(g);
+    if (group)
+      cudaStreamSynchronize(group);
+    drop_graphs();
     cudaFree(d_mask);
     for (Series &se : series) {
       se.lab.reset();
@@ -85,6 +95,12 @@ struct Engine {
       cudaEventDestroy(e);
     for (cudaEvent_t e : consumed)
       cudaEventDestroy(e);
+    for (cudaEvent_t e : placed)
+      cudaEventDestroy(e);
+    for (cudaEvent_t e : grouped)
+      cudaEventDestroy(e);
+    if (join)
+      cudaEventDestroy(join);
     for (cudaEvent_t e : marks)
       if (e)
         cudaEventDestroy(e);
@@ -97,6 +113,21 @@ struct Engine {
       cudaStreamDestroy(compute);
     if (copy)
       cudaStreamDestroy(copy);
+    if (group)
+      cudaStreamDestroy(group);
+  }
+
+  void drop_graphs() {
+    for (cudaGraphExec_t &g : graphs)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
+    for (cudaGraphExec_t &g : thr_graphs)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
   }
 
   void check_slot(int slot) const {
@@ -108,8 +139,8 @@ struct Engine {
       throw std::out_of_range("frame out of range");
   }
 
-  // Threshold, placement and (when enabled) grouping of one slot.
-  void enqueue_body(int slot, cudaEvent_t b, cudaEvent_t c) {
+  // Threshold and placement of one slot, on the compute stream.
+  void enqueue_threshold(int slot, cudaEvent_t b, cudaEvent_t c) {
     if (mask_n)
       check(launch_stamp_mask(plan->frame_origin(slot, 0), plan->elem_bytes(), d_mask, mask_n,
                               compute),
@@ -119,48 +150,106 @@ struct Engine {
       check(cudaEventRecord(c, compute), "cudaEventRecord");
     if (on_mask)
       check(cudaLaunchHostFunc(compute, on_mask, hook_args[slot]), "cudaLaunchHostFunc");
+  }
+
+  // Grouping of one slot's lists, on the group stream.
+  void enqueue_grouping(int slot) {
     for (Series &se : series)
       se.lab->enqueue(se.nframes, plan->out(slot), se.d_offs, plan->frame_count(slot), se.d_map,
-                      se.d_caps, false, compute);
+                      se.d_caps, false, group);
     if (post_run)
       post_run(*this, slot, post_arg);
     if (on_done)
-      check(cudaLaunchHostFunc(compute, on_done, hook_args[slot]), "cudaLaunchHostFunc");
+      check(cudaLaunchHostFunc(group, on_done, hook_args[slot]), "cudaLaunchHostFunc");
+  }
+
+  // Enqueues `body` on `s`, through a graph captured on first use.
+  template <class Body> void replay(cudaGraphExec_t &exec, cudaStream_t s, Body body) {
+    if (!exec) {
+      cudaGraph_t g = nullptr;
+      check(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal),
+            "beginning graph capture");
+      try {
+        body();
+      } catch (...) {
+        cudaStreamEndCapture(s, &g);
+        if (g)
+          cudaGraphDestroy(g);
+        throw;
+      }
+      check(cudaStreamEndCapture(s, &g), "ending graph capture");
+      const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+      cudaGraphDestroy(g);
+      check(e, "instantiating the graph");
+      return; // capturing did not run it
+    }
+    check(cudaGraphLaunch(exec, s), "launching the graph");
   }
 
   void enqueue_run(int slot, cudaEvent_t a, cudaEvent_t b, cudaEvent_t c, cudaEvent_t d) {
+    if (series.empty()) {
+      if (a)
+        check(cudaEventRecord(a, compute), "cudaEventRecord");
+      if (use_graph) {
+        bool fresh = !thr_graphs[slot];
+        replay(thr_graphs[slot], compute, [&] { enqueue_threshold(slot, nullptr, nullptr); });
+        if (fresh)
+          replay(thr_graphs[slot], compute, [] {});
+      } else {
+        enqueue_threshold(slot, b, c);
+      }
+      if (d)
+        check(cudaEventRecord(d, compute), "cudaEventRecord");
+      return;
+    }
+    // the slot's lists are free once its last grouping has read them; when
+    // profiling, the runs are kept apart so each stage times alone
+    check(cudaStreamWaitEvent(compute, grouped[slot], 0), "ordering after the grouping");
+    if (profiling && last_slot >= 0)
+      check(cudaStreamWaitEvent(compute, grouped[last_slot], 0), "ordering after the grouping");
     if (a)
       check(cudaEventRecord(a, compute), "cudaEventRecord");
     if (use_graph) {
+      const bool fresh = !thr_graphs[slot];
+      replay(thr_graphs[slot], compute, [&] { enqueue_threshold(slot, nullptr, nullptr); });
+      if (fresh)
+        replay(thr_graphs[slot], compute, [] {});
+    } else {
+      enqueue_threshold(slot, b, c);
+    }
+    check(cudaEventRecord(placed[slot], compute), "cudaEventRecord");
+    check(cudaStreamWaitEvent(group, placed[slot], 0), "ordering after the placement");
+    if (use_graph) {
       cudaGraphExec_t &exec = graphs[2 * slot + parity];
       if (!exec) {
-        cudaGraph_t g = nullptr;
-        check(cudaStreamBeginCapture(compute, cudaStreamCaptureModeThreadLocal),
-              "beginning graph capture");
-        try {
-          enqueue_body(slot, nullptr, nullptr);
-        } catch (...) {
-          cudaStreamEndCapture(compute, &g);
-          if (g)
-            cudaGraphDestroy(g);
-          throw;
-        }
-        check(cudaStreamEndCapture(compute, &g), "ending graph capture");
-        const cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
-        cudaGraphDestroy(g);
-        check(e, "instantiating the graph");
+        // capturing records the run and flips the host's record of the live
+        // buffers, as the run about to be launched will flip them
+        replay(exec, group, [&] { enqueue_grouping(slot); });
+        replay(exec, group, [] {});
       } else {
+        replay(exec, group, [] {});
         for (Series &se : series)
           se.lab->note_replayed(); // the captured run flips the live buffers too
       }
-      check(cudaGraphLaunch(exec, compute), "launching the graph");
     } else {
-      enqueue_body(slot, b, c);
+      enqueue_grouping(slot);
     }
     if (d)
-      check(cudaEventRecord(d, compute), "cudaEventRecord");
-    if (!series.empty())
-      parity ^= 1;
+      check(cudaEventRecord(d, group), "cudaEventRecord");
+    check(cudaEventRecord(grouped[slot], group), "cudaEventRecord");
+    last_slot = slot;
+    parity ^= 1;
+  }
+
+  // A timing mark after everything enqueued so far, on either stream.
+  void record(cudaEvent_t ev) {
+    if (series.empty()) {
+      check(cudaEventRecord(ev, compute), "cudaEventRecord");
+      return;
+    }
+    check(cudaEventRecord(join, compute), "cudaEventRecord");
+    check(cudaStreamWaitEvent(group, join, 0), "cudaStreamWaitEvent");
+    check(cudaEventRecord(ev, group), "cudaEventRecord");
   }
 
   void run(int slot) {
@@ -225,9 +314,9 @@ struct Engine {
       check(cudaMemcpy(se.d_map, fs.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice), "copy");
       se.lab = std::make_unique<DeviceLabeller>(se.height, se.width, opt);
       se.lab->reserve(total, se.nframes, carry_cap ? carry_cap : 2 * biggest + (1u << 20));
-      se.lab->set_next_frame(first_frame, compute);
+      se.lab->set_next_frame(first_frame, group);
     }
-    check(cudaStreamSynchronize(compute), "cudaStreamSynchronize");
+    check(cudaStreamSynchronize(group), "cudaStreamSynchronize");
     parity = 0;
   }
 
@@ -242,9 +331,9 @@ struct Engine {
   const LabelScalars &group_state(int k) {
     Series &se = series_at(k);
     check(cudaMemcpyAsync(host_sc, se.lab->scalars(), sizeof(LabelScalars),
-                          cudaMemcpyDeviceToHost, compute),
+                          cudaMemcpyDeviceToHost, group),
           "reading the grouping state");
-    check(cudaStreamSynchronize(compute), "cudaStreamSynchronize");
+    check(cudaStreamSynchronize(group), "cudaStreamSynchronize");
     if (host_sc->status != kLabelOk)
       throw DeviceError("grouping capacity exceeded (status " + std::to_string(host_sc->status) +
                         ")");
@@ -292,6 +381,7 @@ struct Engine {
       all.insert(all.end(), f.begin(), f.end());
     check(cudaStreamSynchronize(copy), "cudaStreamSynchronize");
     check(cudaStreamSynchronize(compute), "cudaStreamSynchronize");
+    check(cudaStreamSynchronize(group), "cudaStreamSynchronize");
     cudaFree(d_mask);
     d_mask = nullptr;
     mask_n = 0;
@@ -301,11 +391,7 @@ struct Engine {
             "copying the pixel mask");
       mask_n = all.size();
     }
-    for (cudaGraphExec_t &g : graphs)
-      if (g) {
-        cudaGraphExecDestroy(g);
-        g = nullptr;
-      }
+    drop_graphs();
   }
 
   void upload_chunk(int slot, int frame, const void *chunk, size_t nbytes, int algorithm) {
@@ -324,6 +410,7 @@ struct Engine {
   void synchronize() {
     check(cudaStreamSynchronize(copy), "cudaStreamSynchronize");
     check(cudaStreamSynchronize(compute), "cudaStreamSynchronize");
+    check(cudaStreamSynchronize(group), "cudaStreamSynchronize");
     if (decoder.take_error())
       throw DeviceError("an uploaded chunk held a malformed LZ4 block");
     for (int s = 0; s < plan->nslots(); s++) {
