@@ -69,7 +69,7 @@ struct LabArgs {
   uint32_t *bits, *bcnt;
   uint32_t *comp_root, *msize, *members;
   uint64_t *mpk;
-  uint32_t *runs; // per batch: 2 g for a run's first pixel, 2 g + 1 for a chunk-crossing link
+  uint64_t *runs; // per batch: lab_link's entries, see lab_gather
   Spot *spot_tmp;
   Pixel *pix_tmp;
   uint64_t *pack;
@@ -272,11 +272,17 @@ __global__ void __launch_bounds__(kThreads) lab_gather(LabArgs a) {
       const int first = starts ? 31 - __clz(starts) : 0;
       a.par[g] = static_cast<uint32_t>(base + first);
     }
-    // lab_link's work list: every run's first pixel, and the first lane of
-    // a chunk that a run enters from the chunk before
+    // lab_link's work list: one entry per piece of a run within a chunk --
+    // its first position, its length and whether it continues a run from
+    // the chunk before (lane 0 joined to its left neighbour)
     const bool boundary = left && lane == 0;
     const bool entry = mine && (!left || boundary);
     const uint32_t want = __ballot_sync(kFull, entry);
+    // pieces end at the next piece, at a lane that is not ours, or at the
+    // chunk's end
+    const uint32_t stops = want | ~__ballot_sync(kFull, mine);
+    const uint32_t after = lane == 31 ? 0u : stops & (0xfffffffeu << lane);
+    const uint32_t len = (after ? __ffs(after) - 1 : 32) - lane;
     if (lane == 0)
       warp_count[warp] = __popc(want);
     __syncthreads();
@@ -292,7 +298,7 @@ __global__ void __launch_bounds__(kThreads) lab_gather(LabArgs a) {
     __syncthreads();
     if (entry)
       a.runs[block_at + warp_count[warp] + __popc(want & ((1u << lane) - 1u))] =
-          (static_cast<uint32_t>(g) << 1) | (boundary ? 1u : 0u);
+          g | (static_cast<uint64_t>(len) << 32) | (boundary ? (1ull << 40) : 0ull);
     __syncthreads();
   }
 }
@@ -345,24 +351,17 @@ __global__ void __launch_bounds__(kThreads) lab_link(LabArgs a) {
   // one entry of lab_gather's list per thread, so the lanes of a warp all
   // have a run to link
   for (uint64_t i = gtid(); i < nruns; i += gstride()) {
-    const uint32_t e = a.runs[i];
-    const uint64_t g = e >> 1;
-    if (e & 1u) { // a run crossing into a new chunk
+    const uint64_t e = a.runs[i];
+    const uint64_t g = e & 0xffffffffu;
+    const uint32_t len = static_cast<uint32_t>(e >> 32) & 0x3fu;
+    if (e >> 40) // a run crossing into a new chunk: join the pieces
       uf_unite(a.par, static_cast<uint32_t>(g), static_cast<uint32_t>(g - 1));
-      continue;
-    }
     // the batch's frames are consecutive: a new pixel's frame is its segment
     const int s = first_batch_seg + static_cast<int>(a.fr[g] - z0);
     const uint64_t s0 = a.seg_start[s];
     const uint64_t end = s0 + a.seg_count[s];
     const uint32_t idx = a.ix[g];
-    uint32_t last = idx; // the run's last index
-    for (uint64_t e = g + 1; e < end; e++) {
-      const uint32_t v = a.ix[e];
-      if (v != last + 1 || v % W == 0)
-        break;
-      last = v;
-    }
+    const uint32_t last = idx + len - 1; // the piece's last index (one row, one chunk)
     if (idx >= W)
       unite_overlaps(a, static_cast<uint32_t>(g), table_of(a, s, first_batch_seg), s0, end - s0,
                      idx - W, last - W);

@@ -131,7 +131,7 @@ private:
   uint32_t *bits_ = nullptr, *bcnt_ = nullptr; // bucket bitmaps and their word counts
   uint32_t *comp_root_ = nullptr, *msize_ = nullptr, *members_ = nullptr;
   uint64_t *mpk_ = nullptr; // member offset (low 32) | size-filtered index (high 32)
-  uint32_t *runs_ = nullptr; // lab_link's work list
+  uint64_t *runs_ = nullptr; // lab_link's work list
   Spot *spot_tmp_ = nullptr;  // spots by size-filtered index, before acceptance
   Pixel *pix_tmp_ = nullptr;  // their pixels, by member offset
   uint64_t *pack_ = nullptr;
