@@ -19,9 +19,10 @@
 //     8-bit rows, then horizontal AND with 2 shuffled neighbour bits);
 //   - vertical 11-row running sums of the count+sum of pixels that are valid
 //     and not kept by the erode, from rows r-5 and r-16;
-//   - at row r-10, for the rare pixels that are candidates (value > 0 and
-//     kept by the erode), the 11 x 11 window by a horizontal pass, the
-//     Poisson test, and the emit of a SignalPixel into a staging pool.
+//   - at row r-10, for the pixels that are candidates (value > 0 and kept
+//     by the erode), compacted one per lane, the 11 x 11 window as the sum
+//     of 11 columns' vertical sums from shared memory, the Poisson test,
+//     and the emit of a SignalPixel into a staging pool.
 // Every window is the reference's window clipped to the frame: the arena
 // holds the masked sentinel everywhere outside the frame, and a pixel off the
 // frame and a masked pixel are treated identically by every step of the
@@ -64,6 +65,7 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr uint32_t kNoChunk = 0xffffffffu;
+constexpr int kRadius11 = 5; // the background window is 11 x 11
 
 template <typename T> struct Real;
 template <> struct Real<uint16_t> { using type = float; };
@@ -343,7 +345,7 @@ __global__ void __launch_bounds__(WPC * 32, (sizeof(T) == 2 ? 16 : 8) / WPC)
   __shared__ Rl sqrt_tab[64];
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  // Per warp: the ring, the 11 x 11 window sums of one row (for the
+  // Per warp: the ring, the 11-row vertical sums of one row (for the
   // candidates), the stage barriers and the candidate column list.
   unsigned char *at = smem_raw;
   T *ring = reinterpret_cast<T *>(at + warp * (kRowBytes * kRingRows));
@@ -543,13 +545,12 @@ __global__ void __launch_bounds__(WPC * 32, (sizeof(T) == 2 ? 16 : 8) / WPC)
         const uint32_t cs = static_cast<uint32_t>(hist_cs >> 40) & 0xffu & outmask;
         if (__any_sync(kFull, cs != 0)) {
           // The candidates are compacted one per lane before the Poisson
-          // test, so each pays for one division and one square root
-          // instead of every lane paying for all eight columns.
-          A hg[8];
-          hsum<5>(vg, hg);
+          // test, so each pays for one division and one square root -- and
+          // for one 11-column sum of the vertical sums, read from shared
+          // memory -- instead of every lane paying for all eight columns.
 #pragma unroll
           for (int k = 0; k < 8; k++)
-            win11[8 * lane + k] = hg[k];
+            win11[8 * lane + k] = vg[k];
           // The candidate columns in ascending order: lane by lane, and
           // within a lane by column.
           const uint32_t cnt = __popc(cs);
@@ -596,9 +597,12 @@ __global__ void __launch_bounds__(WPC * 32, (sizeof(T) == 2 ? 16 : 8) / WPC)
             bool sig = false;
             SignalPixel px;
             if (i < total) {
-              const uint32_t col = cand_col[i];
+              const uint32_t col = cand_col[i]; // an output column: col +- 5 is in the strip
               const uint32_t p = prow[col];
-              const A h = win11[col];
+              A h = 0;
+#pragma unroll
+              for (int d = -kRadius11; d <= kRadius11; d++)
+                h += win11[col + d];
               if (p > 0) { // a masked pixel is never a candidate
                 sig = poisson(p, h >> Tr::kShift11, h & (C11 - 1), &px.background);
                 px.index = row_index + col;
