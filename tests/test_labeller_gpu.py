@@ -160,3 +160,29 @@ def test_threshold_then_group_4m(gpu_lib):
     for img, sig in zip(frames, sigs):
         assert sig.tobytes() == O.dext(img)[1].tobytes()
     assert_same(sigs, *frames[0].shape)
+
+
+def test_components_of_every_size_class(gpu_lib):
+    """Components handled by each path of the spot pass: up to 512 members,
+    512 to 1024 (the large-buffer launch) and beyond 1024 (through global
+    memory, reachable with max_spot_size above 1024), with uneven values so
+    that the doubles depend on the member order, and bright enough that the
+    first pass can not be summed in parallel exactly."""
+    rng = np.random.default_rng(5)
+    h, w = 120, 160
+    sigs = []
+    for z in range(4):
+        idx = []
+        for y0, x0, side in ((5, 5, 10), (30, 40, 15), (70, 20, 24), (60, 100, 30)):
+            ys, xs = np.mgrid[y0:y0 + side, x0:x0 + side]
+            idx.append((ys * w + xs).ravel())
+        idx = np.unique(np.concatenate(idx))
+        sig = np.zeros(len(idx), O.SIGNAL_PIXEL)
+        sig["index"] = idx
+        sig["value"] = rng.integers(1, 0xFFFE, len(idx))
+        sig["value"][::97] = 4_000_000_000  # 32-bit values: inexact parallel sums
+        sigs.append(sig)
+    spots = assert_same(sigs, h, w, max_spot_size=100000, max_separation=0.0)
+    sizes = sorted(int(s["n_signal"]) for s in spots)
+    assert sizes == [400, 900, 2304, 3600]  # 4 frames of 10^2, 15^2, 24^2 and 30^2
+    assert_same(sigs, h, w, max_spot_size=100000, max_separation=2.0)

@@ -132,3 +132,18 @@ def test_pixel_mask_in_a_served_series(gpu_lib):
         f[mask] = 0xFFFF
         stamped.append(f)
     check_oracle(stamped, two_d, *got)
+
+
+def test_u32_series_served(gpu_lib):
+    from dials_metal_spotfinder_b200 import synth
+    from dials_metal_spotfinder_b200.serve import Server
+    s = synth.Series(300, 420, 8, 0x5EED0042, dtype=np.uint32, gaps=False, ring_r0=150.0,
+                     spots_per_frame=40.0, intensity=(50.0, 2.0e6))
+    frames = [s.frame(z) for z in range(s.frames)]
+    with Server() as srv:
+        sid = srv.open(frames[0].shape, dtype=np.uint32)
+        for c in encode_all(frames):
+            assert srv.submit(sid, c, timeout_s=30)
+        srv.finish(sid)
+        got = results(srv, sid)
+    check_oracle(frames, False, *got)
