@@ -58,7 +58,7 @@ def parse():
     # ten frames here): a reflection present at both ends of a short cycle
     # would be joined across the wrap into a streak that never closes.
     ap.add_argument("--pool", type=int, default=32, help="distinct synthetic frames")
-    ap.add_argument("--e2e-steps", type=int, default=4)
+    ap.add_argument("--e2e-steps", type=int, default=8)
     ap.add_argument("--cpu-frames", type=int, default=8)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=3.0,
@@ -327,36 +327,54 @@ def run_ours(args, ranks):
     peak, peak_kind = measured_peaks()
     traffic = recorded_traffic().get(f"threshold_u16_{SHAPE[0]}x{SHAPE[1]}_per_frame")
 
-    # e2e: pinned host frames -> device -> signal lists back, per step
+    # e2e: pinned host frames -> device -> the finished spots and their
+    # pixels back into pinned host memory, every step. Pipelined the way a
+    # user drives the engine: step i+1's frames stream in on the copy engine
+    # while step i computes and its results come back on the other direction
+    # of the link.
     e2e = None
     if args.e2e_steps > 0:
         hb = [sf.HostBuffer(SHAPE, np.uint16) for _ in range(F)]
         for f in range(F):
             hb[f].array[:] = pool[f % len(pool)]
-        d2h = 0
 
-        def e2e_step(slot):
-            # frames in from pinned host memory; the step's finished spots and
-            # their pixels back to the host
-            nonlocal d2h
+        def e2e_upload(slot):
             for f in range(F):
                 eng.upload(slot, f, hb[f].array)
-            eng.run(slot)
-            spots = eng.spots()
-            pixels = eng.pixels()
-            d2h = spots.nbytes + pixels.nbytes
-        e2e_step(0)
+
+        # result buffers sized from one untimed step
+        e2e_upload(0)
+        eng.run(0)
+        n_spots, n_pix = len(eng.spots()), len(eng.pixels())
+        spot_buf = sf.HostBuffer((2 * n_spots + (1 << 16),), sf.SPOT)
+        pix_buf = sf.HostBuffer((2 * n_pix + (1 << 20),), sf.PIXEL)
+        d2h = []
+
+        def e2e_read():
+            sp = eng.spots(out=spot_buf.array)
+            px = eng.pixels(out=pix_buf.array)
+            d2h.append(sp.nbytes + px.nbytes)
+
         eng.synchronize()
         ranks.barrier()
         t0 = time.perf_counter()
-        for i in range(args.e2e_steps):
-            e2e_step(i % 2)
+        e2e_upload(0)
+        eng.run(0)
+        for i in range(1, args.e2e_steps):
+            e2e_upload(i % 2)
+            e2e_read()          # step i-1, overlapping step i's upload
+            eng.run(i % 2)
+        e2e_read()
         eng.synchronize()
         dt = ranks.max(time.perf_counter() - t0)
         e2e = {"value": ranks.sum(F * args.e2e_steps) / dt, "unit": UNIT,
-               "h2d_bytes_per_step": F * frame_bytes, "d2h_bytes_per_step": d2h,
-               "timer": "host wall clock, synchronised at both ends"}
-        for b in hb:
+               "h2d_bytes_per_step": F * frame_bytes,
+               "d2h_bytes_per_step": int(statistics.mean(d2h)),
+               "timer": "host wall clock, synchronised at both ends",
+               "form": "Engine.upload from pinned host frames, run, spots/pixels into "
+                       "pinned host arrays; step i+1 uploads while step i computes and "
+                       "reads back"}
+        for b in hb + [spot_buf, pix_buf]:
             b.close()
 
     # the plain per-frame GPU form, the same frame through sf_find_u16
@@ -364,15 +382,18 @@ def run_ours(args, ranks):
     if ranks.rank == 0:
         hb0 = sf.HostBuffer(SHAPE, np.uint16)
         hb0.array[:] = pool[0]
+        sig0 = sf.HostBuffer((SHAPE[0] * SHAPE[1] * 2 // 16,), sf.SIGNAL_PIXEL)
         for _ in range(2):
-            sf.find(hb0.array)
+            sf.find(hb0.array, out=sig0.array)
         t0 = time.perf_counter()
         nplain = 10
         for _ in range(nplain):
-            sf.find(hb0.array)
+            sf.find(hb0.array, out=sig0.array)
         plain = {"value": nplain / (time.perf_counter() - t0), "unit": UNIT,
-                 "form": "sf_find_u16, one frame per call from pinned host memory"}
+                 "form": "sf_find_u16, one frame per call, pinned host frame and "
+                         "pinned signal list"}
         hb0.close()
+        sig0.close()
 
     ref_gpu = None
     if ranks.rank == 0:
@@ -476,19 +497,21 @@ def batched_vs_plain_4m(steps: int = 10):
         batched = F * steps / (eng.elapsed_ms(0, 1) / 1e3)
     hb = sf.HostBuffer(shape, np.uint16)
     hb.array[:] = pool[0]
+    sig = sf.HostBuffer((shape[0] * shape[1] * 2 // 16,), sf.SIGNAL_PIXEL)
     for _ in range(3):
-        sf.find(hb.array)
+        sf.find(hb.array, out=sig.array)
     n = 30
     t0 = time.perf_counter()
     for i in range(n):
-        sf.find(hb.array)
+        sf.find(hb.array, out=sig.array)
     plain = n / (time.perf_counter() - t0)
     hb.close()
+    sig.close()
     return {"workload": "4M-shaped uint16 frames, 2162x2068", "unit": UNIT,
             "batched": batched, "plain": plain, "ratio": batched / plain,
             "batched_form": "engine, 16 frames per launch, resident, threshold + 3D grouping, "
                             "graph replay, CUDA events",
-            "plain_form": "sf_find_u16 per frame from pinned host memory, threshold only, "
+            "plain_form": "sf_find_u16 per frame, pinned frame and signal list, threshold only, "
                           "host wall clock"}
 
 

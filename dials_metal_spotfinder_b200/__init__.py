@@ -52,6 +52,9 @@ def find_status(image: np.ndarray, out: np.ndarray | None = None):
     signal than the device list holds); ``signal`` is the SignalPixel array
     ascending by index (empty unless status is 0). A device failure raises
     DeviceError, as the reference's std::runtime_error does.
+
+    ``out``, a SIGNAL_PIXEL array of at least height*width*itemsize/16
+    records, receives the list and ``signal`` is then a view into it.
     """
     if image is None or image.ndim != 2 or image.dtype not in (np.uint16, np.uint32):
         return -1, np.zeros(0, SIGNAL_PIXEL)
@@ -60,7 +63,11 @@ def find_status(image: np.ndarray, out: np.ndarray | None = None):
     if h == 0 or w == 0:
         return -1, np.zeros(0, SIGNAL_PIXEL)
     cap = max(_capacity(image), 1)
-    if out is None or len(out) < cap:
+    given = out is not None and len(out) >= cap
+    if given:
+        if out.dtype != SIGNAL_PIXEL or out.ndim != 1 or not out.flags.c_contiguous:
+            return -1, np.zeros(0, SIGNAL_PIXEL)
+    else:
         out = np.empty(cap, SIGNAL_PIXEL)
     found = ctypes.c_size_t(0)
     fn = lib.sf_find_u16 if image.dtype == np.uint16 else lib.sf_find_u32
@@ -69,12 +76,15 @@ def find_status(image: np.ndarray, out: np.ndarray | None = None):
         raise_for(status, "find")
     if status != 0:
         return status, np.zeros(0, SIGNAL_PIXEL)
-    return 0, out[: found.value].copy()
+    # into the caller's array (a HostBuffer's page-locked one copies fastest)
+    # a view of the filled part; otherwise a compact copy
+    return 0, out[: found.value] if given else out[: found.value].copy()
 
 
-def find(image: np.ndarray) -> np.ndarray:
-    """Threshold one frame; raises BadArgument / Overflow / DeviceError."""
-    status, signal = find_status(image)
+def find(image: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:
+    """Threshold one frame; raises BadArgument / Overflow / DeviceError.
+    `out` as for find_status."""
+    status, signal = find_status(image, out)
     raise_for(status, "find")
     return signal
 
@@ -101,15 +111,16 @@ class HostBuffer:
         dtype = np.dtype(dtype)
         nbytes = int(np.prod(shape)) * dtype.itemsize
         self._ptr = lib.sf_host_alloc(max(nbytes, 1))
+        self._free = lib.sf_host_free  # still bound when module globals are gone at exit
         if not self._ptr:
             raise DeviceError("sf_host_alloc failed")
         buf = (ctypes.c_char * max(nbytes, 1)).from_address(self._ptr)
         self.array = np.frombuffer(buf, dtype=dtype, count=int(np.prod(shape))).reshape(shape)
 
     def close(self):
-        if self._ptr:
+        if getattr(self, "_ptr", None):
             self.array = None
-            lib.sf_host_free(self._ptr)
+            self._free(self._ptr)
             self._ptr = None
 
     def __del__(self):

@@ -92,6 +92,7 @@ SIGNATURES = {
     "sf_chunk_bound": (_S, [_S, _S, _I]),
     "sf_chunk_encode": (_I, [_I, _P, _S, _S, _I, _P, _S, ctypes.POINTER(_S)]),
     "sf_chunk_decode": (_I, [_I, _P, _S, _S, _S, _I, _P]),
+    "sf_chunk_decode_device": (_I, [_I, _P, _S, _S, _S, _I, _P, _S]),
     "sf_server_create": (_I, [_P, ctypes.POINTER(_P)]),
     "sf_server_destroy": (None, [_P]),
     "sf_server_open": (_I, [_P, _S, _S, _I, _P, ctypes.c_int64, ctypes.POINTER(_I)]),

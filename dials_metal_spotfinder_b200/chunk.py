@@ -2,7 +2,7 @@
 reference's decompress::image, src/decompress.hh:14-31): frames as the HDF5
 filters store them, uncompressed ("raw"), "lz4" or "bslz4" (bitshuffle +
 LZ4). encode() is the detector / replay side, decode() the host decoder;
-Engine.upload_chunk() decodes on the device."""
+decode_device() and Engine.upload_chunk() decode on the device."""
 
 from __future__ import annotations
 
@@ -43,3 +43,16 @@ def decode(chunk, shape, dtype=np.uint16, algorithm="bslz4") -> np.ndarray:
     raise_for(lib.sf_chunk_decode(algorithm_code(algorithm), chunk.ctypes.data, len(chunk), h, w,
                                   np.dtype(dtype).itemsize, out.ctypes.data), "chunk.decode")
     return out
+
+
+def decode_device(chunk, shape, dtype, device_ptr: int, pitch_bytes: int | None = None,
+                  algorithm="bslz4") -> None:
+    """Decodes `chunk` on the device into device memory at `device_ptr`
+    (rows `pitch_bytes` apart, default the row length); waits for it."""
+    chunk = np.ascontiguousarray(np.frombuffer(chunk, np.uint8) if isinstance(chunk, bytes)
+                                 else chunk, dtype=np.uint8)
+    h, w = shape
+    eb = np.dtype(dtype).itemsize
+    pitch = w * eb if pitch_bytes is None else int(pitch_bytes)
+    raise_for(lib.sf_chunk_decode_device(algorithm_code(algorithm), chunk.ctypes.data, len(chunk),
+                                         h, w, eb, device_ptr, pitch), "chunk.decode_device")

@@ -344,10 +344,14 @@ int sf_engine_series_spots(sf_engine *engine, int series, sf_spot *out, size_t c
     *n = s.batch_spots;
     if (s.batch_spots > capacity)
       return -2;
-    if (s.batch_spots)
-      sf::check(cudaMemcpy(out, e->series[series].lab->batch_spots(),
-                           s.batch_spots * sizeof(sf::Spot), cudaMemcpyDeviceToHost),
+    if (s.batch_spots) {
+      // on the grouping stream, after the run that made them: a DMA straight
+      // into page-locked memory, while the copy stream's uploads continue
+      sf::check(cudaMemcpyAsync(out, e->series[series].lab->batch_spots(),
+                                s.batch_spots * sizeof(sf::Spot), cudaMemcpyDeviceToHost, e->group),
                 "reading spots");
+      sf::check(cudaStreamSynchronize(e->group), "cudaStreamSynchronize");
+    }
     return 0;
   });
 }
@@ -362,10 +366,14 @@ int sf_engine_series_pixels(sf_engine *engine, int series, sf_pixel *out, size_t
     *n = s.batch_pixels;
     if (s.batch_pixels > capacity)
       return -2;
-    if (s.batch_pixels)
-      sf::check(cudaMemcpy(out, e->series[series].lab->batch_pixels(),
-                           s.batch_pixels * sizeof(sf::Pixel), cudaMemcpyDeviceToHost),
+    if (s.batch_pixels) {
+      // on the grouping stream, after the run that made them: a DMA straight
+      // into page-locked memory, while the copy stream's uploads continue
+      sf::check(cudaMemcpyAsync(out, e->series[series].lab->batch_pixels(),
+                                s.batch_pixels * sizeof(sf::Pixel), cudaMemcpyDeviceToHost, e->group),
                 "reading spot pixels");
+      sf::check(cudaStreamSynchronize(e->group), "cudaStreamSynchronize");
+    }
     return 0;
   });
 }

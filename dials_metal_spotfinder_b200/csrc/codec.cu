@@ -278,6 +278,13 @@ ChunkLayout parse_chunk(int algorithm, const uint8_t *data, size_t nbytes, size_
   size_t at = kHeader;
   size_t done = 0; // decoded bytes so far
   const size_t coded = algorithm == SF_CHUNK_BSLZ4 ? (n_elems - n_elems % 8) * s : bytes;
+  // the block count follows from the header; a chunk that claims more
+  // blocks than it has bytes for fails below, so bound the reservation
+  const size_t expect = std::min<size_t>((coded + block_bytes - 1) / block_bytes, nbytes / 5 + 1);
+  L.block_in.reserve(expect);
+  L.block_len.reserve(expect);
+  L.block_out.reserve(expect);
+  L.block_n.reserve(expect);
   while (done < coded) {
     if (at + 4 > nbytes)
       throw std::invalid_argument("chunk truncated");

@@ -206,6 +206,9 @@ struct Server {
     std::vector<ThresholdPlan::Shape> shapes{{static_cast<int32_t>(h), static_cast<int32_t>(w)}};
     se->eng = make_engine(eb, shapes, PlanTuning{}, slots);
     se->eng->enable_grouping(opt, first_frame, 0);
+    // the decoder's staging sets, sized for the largest chunk of this shape
+    // with 8 KB blocks, count toward the series' device bytes
+    se->eng->decoder.reserve(sf_chunk_bound(h, w, eb), (h * w * eb + 8191) / 8192 + 1);
     size_t free1 = 0;
     check(cudaMemGetInfo(&free1, &total), "cudaMemGetInfo");
     se->device_bytes = free0 > free1 ? free0 - free1 : 0;

@@ -36,12 +36,18 @@ ChunkLayout parse_chunk(int algorithm, const uint8_t *data, size_t nbytes, size_
                         size_t elem);
 void decode_chunk_host(const uint8_t *data, const ChunkLayout &L, uint8_t *out);
 
-// Decodes chunks into device frames (decode.cu): the chunk's bytes and its
-// block table go to the device, one warp decodes each LZ4 block (and undoes
-// the bit transpose in shared memory), and the frame lands at `dst` with
-// row pitch `dst_pitch`. Staging buffers grow as needed and are reused; the
-// work is ordered on the stream it is given, so one decoder serves one
-// stream. A malformed block sets a sticky device flag, read by
+// Brings frames from host memory into device frames (decode.cu): compressed
+// chunks (their bytes and block table go to the device, one warp decodes
+// each LZ4 block in shared memory and undoes the bit transpose, and writes
+// the elements straight into `dst` at row pitch `dst_pitch`) and raw frames
+// (one contiguous copy, then laid out at the pitch by a kernel).
+//
+// Host-to-device copies run on the decoder's own stream into a ring of
+// staging sets, so frame k+1 crosses the link while frame k is decoded; the
+// decode itself is ordered on the stream the caller gives, so one decoder
+// serves one stream and work on that stream after enqueue() sees the frame.
+// The caller keeps its host buffer unchanged until that stream has passed
+// the frame. A malformed block sets a sticky device flag, read by
 // take_error().
 class DeviceChunkDecoder {
 public:
@@ -52,18 +58,39 @@ public:
 
   void enqueue(const uint8_t *chunk, size_t nbytes, const ChunkLayout &L, size_t height,
                size_t width, void *dst, size_t dst_pitch, cudaStream_t s);
+  // A raw frame of height rows of row_bytes each, contiguous at `src` (host
+  // or device memory).
+  void enqueue_raw(const void *src, size_t height, size_t row_bytes, void *dst, size_t dst_pitch,
+                   cudaStream_t s);
+  // Allocates every staging set for chunks up to `chunk_bytes` with up to
+  // `blocks` LZ4 blocks, so later calls allocate nothing.
+  void reserve(size_t chunk_bytes, size_t blocks);
   // Whether a block failed since the last call (synchronises the device).
   bool take_error();
   // The device flag itself (nonzero after a failed block), allocated and
   // cleared on first use.
   int *error_flag();
 
+  static constexpr int kSets = 3;
+
 private:
-  uint8_t *d_chunk_ = nullptr;
-  size_t chunk_cap_ = 0;
-  void *d_blocks_ = nullptr;
-  size_t blocks_cap_ = 0;
-  uint8_t *d_linear_ = nullptr;
+  struct Set {
+    uint8_t *d_in = nullptr; // the chunk (or raw frame) on the device
+    size_t in_cap = 0;
+    void *h_table = nullptr; // block table, page-locked, and its device copy
+    void *d_table = nullptr;
+    size_t table_cap = 0;    // entries
+    cudaEvent_t copied = nullptr; // the set's host-to-device copies are done
+    cudaEvent_t freed = nullptr;  // the decode that read the set is done
+    bool used = false;
+  };
+  Set &next_set(size_t in_bytes, size_t entries);
+  void prepare();
+
+  Set sets_[kSets];
+  int next_ = 0;
+  cudaStream_t h2d_ = nullptr;
+  uint8_t *d_linear_ = nullptr; // a frame decoded from blocks beyond shared memory
   size_t linear_cap_ = 0;
   int *d_err_ = nullptr;
 };

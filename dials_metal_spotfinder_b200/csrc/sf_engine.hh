@@ -344,7 +344,12 @@ struct Engine {
     check_slot(slot);
     check_frame(frame);
     check(cudaStreamWaitEvent(copy, consumed[slot], 0), "ordering after the last run");
-    plan->upload(slot, frame, host, copy);
+    // one contiguous copy on the decoder's stream (the next frame's overlaps
+    // this one's placement), laid out at the arena's pitch on `copy`
+    const ThresholdPlan::Shape &sh = plan->shape(frame);
+    const size_t eb = static_cast<size_t>(plan->elem_bytes());
+    decoder.enqueue_raw(host, sh.height, static_cast<size_t>(sh.width) * eb,
+                        plan->frame_origin(slot, frame), plan->pitch() * eb, copy);
     check(cudaEventRecord(uploaded[slot], copy), "cudaEventRecord");
   }
 

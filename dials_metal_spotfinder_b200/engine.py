@@ -166,28 +166,33 @@ class Engine:
                   "group_counts")
         return dict(zip(COUNT_NAMES, (int(v) for v in out))), int(live.value)
 
-    def spots(self, series: int = 0) -> np.ndarray:
-        """Spots of a series finished by the last run (or by finish())."""
+    def _records(self, fn, series, dtype, out, what):
         n = ctypes.c_size_t(0)
-        status = lib.sf_engine_series_spots(self._h, series, None, 0, ctypes.byref(n))
+        if out is not None:
+            if out.dtype != dtype or out.ndim != 1 or not out.flags.c_contiguous:
+                raise ValueError(f"out must be a contiguous 1-D array of {what} records")
+            raise_for(fn(self._h, series, out.ctypes.data if len(out) else None, len(out),
+                         ctypes.byref(n)), what)
+            return out[:n.value]
+        status = fn(self._h, series, None, 0, ctypes.byref(n))
         if status not in (0, -2):
-            raise_for(status, "spots")
-        out = np.zeros(n.value, SPOT)
-        raise_for(lib.sf_engine_series_spots(self._h, series,
-                                             out.ctypes.data if n.value else None, n.value,
-                                             ctypes.byref(n)), "spots")
+            raise_for(status, what)
+        out = np.zeros(n.value, dtype)
+        raise_for(fn(self._h, series, out.ctypes.data if n.value else None, n.value,
+                     ctypes.byref(n)), what)
         return out
 
-    def pixels(self, series: int = 0) -> np.ndarray:
-        n = ctypes.c_size_t(0)
-        status = lib.sf_engine_series_pixels(self._h, series, None, 0, ctypes.byref(n))
-        if status not in (0, -2):
-            raise_for(status, "pixels")
-        out = np.zeros(n.value, PIXEL)
-        raise_for(lib.sf_engine_series_pixels(self._h, series,
-                                              out.ctypes.data if n.value else None, n.value,
-                                              ctypes.byref(n)), "pixels")
-        return out
+    def spots(self, series: int = 0, out: np.ndarray | None = None) -> np.ndarray:
+        """Spots of a series finished by the last run (or by finish()).
+
+        With `out` (a SPOT array, best a HostBuffer's page-locked one) the
+        records are copied into it and a view of the filled part returned;
+        Overflow if it is too short."""
+        return self._records(lib.sf_engine_series_spots, series, SPOT, out, "spots")
+
+    def pixels(self, series: int = 0, out: np.ndarray | None = None) -> np.ndarray:
+        """The finished spots' pixels, in spot order; `out` as for spots()."""
+        return self._records(lib.sf_engine_series_pixels, series, PIXEL, out, "pixels")
 
     def finish(self) -> None:
         raise_for(lib.sf_engine_finish(self._h), "finish")

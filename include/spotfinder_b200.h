@@ -191,6 +191,15 @@ SF_API int sf_chunk_encode(int algorithm, const void *image, size_t height, size
                            int elem_bytes, void *out, size_t capacity, size_t *written);
 SF_API int sf_chunk_decode(int algorithm, const void *chunk, size_t nbytes, size_t height,
                            size_t width, int elem_bytes, void *image);
+/* The device decoder on its own: `chunk` (host memory) decoded into device
+ * memory at `device_image`, rows `pitch_bytes` apart (at least width *
+ * elem_bytes), one warp per LZ4 block. Waits for the decode. Returns as
+ * sf_chunk_decode, or -3 for a device failure, a malformed LZ4 block found
+ * on the device included. The batched engine's sf_engine_upload_chunk uses
+ * the same decoder. */
+SF_API int sf_chunk_decode_device(int algorithm, const void *chunk, size_t nbytes, size_t height,
+                                  size_t width, int elem_bytes, void *device_image,
+                                  size_t pitch_bytes);
 
 /* ---- the reflection table: src/refl.hh:72-74 (refl::write) ------------- *
  *

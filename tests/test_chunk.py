@@ -224,3 +224,89 @@ def test_device_reports_a_malformed_block(gpu_lib):
         eng.upload_chunk(0, 0, good)  # and the engine still works
         eng.run(0)
         eng.synchronize()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("algorithm", ["raw", "lz4", "bslz4"])
+@pytest.mark.parametrize("dtype", [np.uint16, np.uint32])
+def test_device_decode_is_exact(gpu_lib, algorithm, dtype):
+    """Every byte of the decoded frame, at a pitch wider than the row and at
+    the row's own length: widths whose rows end inside a group of eight
+    elements, single columns, frames shorter than one block, a raw tail."""
+    import torch
+    rng = np.random.default_rng(11)
+    shapes = [(1, 1), (3, 5), (7, 3), (1, 9), (41, 465), (257, 511), (300, 4148 // 4),
+              (1062, 1028), (64, 4099)]
+    for h, w in shapes:
+        img = rng.poisson(1.5, (h, w)).astype(dtype)
+        img[rng.random((h, w)) < 0.01] = np.iinfo(dtype).max
+        img[rng.random((h, w)) < 0.005] = rng.integers(1000, 60000)
+        ch = C.encode(img, algorithm)
+        eb = img.dtype.itemsize
+        for pitch in (w * eb, ((w * eb + 127) // 128) * 128 + 16):
+            dev = torch.full((h * pitch,), 0xA5, dtype=torch.uint8, device="cuda")
+            C.decode_device(ch, img.shape, dtype, dev.data_ptr(), pitch, algorithm)
+            got = dev.cpu().numpy().reshape(h, pitch)
+            rows = got[:, : w * eb].copy().view(dtype)
+            assert np.array_equal(rows, img), (algorithm, h, w, pitch)
+            # the bytes between rows are untouched
+            assert (got[:, w * eb:] == 0xA5).all(), (algorithm, h, w, pitch)
+
+
+@pytest.mark.gpu
+def test_device_decode_16m_frame(gpu_lib):
+    import torch
+    from dials_metal_spotfinder_b200 import synth
+    img = synth.eiger_16m(frames=1).frame(0)
+    h, w = img.shape
+    ch = C.encode(img, "bslz4")
+    dev = torch.empty((h, 4224), dtype=torch.uint16, device="cuda")
+    C.decode_device(ch, img.shape, np.uint16, dev.data_ptr(), 4224 * 2)
+    assert np.array_equal(dev[:, :w].cpu().numpy(), img)
+
+
+@pytest.mark.gpu
+def test_device_decode_refuses_a_malformed_block(gpu_lib):
+    import torch
+    from dials_metal_spotfinder_b200._lib import DeviceError
+    rng = np.random.default_rng(3)
+    img = rng.poisson(2.0, (256, 384)).astype(np.uint16)
+    good = C.encode(img, "bslz4")
+    size, block, parts, rest = split_blocks(bytes(good), img.nbytes)
+    first = bytes([0x0F, 0xFF, 0xFF]) + parts[0][3:]
+    bad = bytearray(good[:12]) + struct.pack(">I", len(first)) + first
+    bad += bytes(good[12 + 4 + len(parts[0]):])
+    dev = torch.empty(img.shape, dtype=torch.uint16, device="cuda")
+    with pytest.raises(DeviceError):
+        C.decode_device(np.frombuffer(bytes(bad), np.uint8), img.shape, np.uint16, dev.data_ptr())
+    C.decode_device(good, img.shape, np.uint16, dev.data_ptr())
+    assert np.array_equal(dev.cpu().numpy(), img)
+
+
+@pytest.mark.gpu
+@needs_liblz4
+@pytest.mark.parametrize("block", [65536, 0])
+def test_device_decode_large_lz4_blocks(gpu_lib, block):
+    """Plain LZ4 chunks whose blocks exceed shared memory (HDF5's LZ4 filter
+    writes up to 1 GB blocks; 0 here: the whole frame in one block), made by
+    liblz4, decode on the device exactly as on the host."""
+    import torch
+    rng = np.random.default_rng(8)
+    img = rng.poisson(0.8, (517, 1031)).astype(np.uint16)
+    img[::9, ::4] = 3000
+    raw = img.reshape(-1).view(np.uint8).tobytes()
+    bs = block or len(raw)
+    out = bytearray(struct.pack(">QI", len(raw), bs))
+    for at in range(0, len(raw), bs):
+        src = raw[at:at + bs]
+        dst = ctypes.create_string_buffer(len(src) + len(src) // 255 + 64)
+        cs = LZ4.LZ4_compress_default(src, dst, len(src), len(dst))
+        assert cs > 0
+        out += struct.pack(">I", cs) + dst.raw[:cs]
+    ch = np.frombuffer(bytes(out), np.uint8)
+    assert np.array_equal(C.decode(ch, img.shape, np.uint16, "lz4"), img)
+    pitch = 1031 * 2 + 50
+    dev = torch.zeros((517 * pitch,), dtype=torch.uint8, device="cuda")
+    C.decode_device(ch, img.shape, np.uint16, dev.data_ptr(), pitch, "lz4")
+    got = dev.cpu().numpy().reshape(517, pitch)[:, :1031 * 2].copy().view(np.uint16)
+    assert np.array_equal(got, img)

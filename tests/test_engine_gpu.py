@@ -139,3 +139,44 @@ def test_engine_grouping_4m(gpu_lib):
     assert counts == want.counts
     same_spots(spots, want.spots)
     assert pixels.tobytes() == want.pixels.tobytes()
+
+
+def test_results_into_pinned_arrays(gpu_lib):
+    """spots()/pixels() into caller arrays (page-locked here) give the same
+    records as the allocating form, while the next run's frames upload; an
+    array too short raises Overflow."""
+    import dials_metal_spotfinder_b200 as sf
+    from dials_metal_spotfinder_b200 import synth
+    from dials_metal_spotfinder_b200.engine import Engine
+    series = synth.small()
+    frames = [series.frame(f) for f in range(6)]
+    ref_spots, ref_pixels, _ = run_series_through_engine(frames, 2, False)
+    sb = sf.HostBuffer((len(ref_spots) + 16,), sf.SPOT)
+    pb = sf.HostBuffer((len(ref_pixels) + 16,), sf.PIXEL)
+    spots, pixels = [], []
+    try:
+        with Engine([frames[0].shape] * 2, frames[0].dtype, slots=2) as eng:
+            eng.enable_grouping(first_frame=0)
+            for f in range(2):
+                eng.upload(0, f, frames[f])
+            eng.run(0)
+            for b in (1, 2):
+                for f in range(2):
+                    eng.upload(b % 2, f, frames[2 * b + f])
+                spots.append(eng.spots(out=sb.array).copy())
+                pixels.append(eng.pixels(out=pb.array).copy())
+                eng.run(b % 2)
+            spots.append(eng.spots(out=sb.array).copy())
+            pixels.append(eng.pixels(out=pb.array).copy())
+            eng.finish()
+            n = len(eng.pixels())
+            if n:
+                with pytest.raises(sf.Overflow):
+                    eng.pixels(out=np.zeros(n - 1, sf.PIXEL))
+            spots.append(eng.spots(out=sb.array).copy())
+            pixels.append(eng.pixels(out=pb.array).copy())
+    finally:
+        sb.close()
+        pb.close()
+    assert np.concatenate(spots).tobytes() == ref_spots.tobytes()
+    assert np.concatenate(pixels).tobytes() == ref_pixels.tobytes()

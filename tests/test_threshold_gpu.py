@@ -154,3 +154,20 @@ def test_concurrent_threads(gpu_lib):
     with ThreadPoolExecutor(6) as pool:
         for z, got in pool.map(run, list(range(len(frames))) * 3):
             same(got, signals[z], f"thread frame {z}")
+
+
+def test_find_into_pinned_list(gpu_lib):
+    """The list written into a caller's page-locked array is the same list,
+    returned as a view of it; an array of the wrong record type is refused."""
+    g = load_golden("threshold_u16.npz")
+    img = g["frame0"]
+    cap = img.shape[0] * img.shape[1] * 2 // 16
+    buf = gpu_lib.HostBuffer((cap,), gpu_lib.SIGNAL_PIXEL)
+    try:
+        got = gpu_lib.find(img, out=buf.array)
+        assert np.shares_memory(got, buf.array)
+        same(got, as_records(g["signal0"], O.SIGNAL_PIXEL), "pinned")
+        status, _ = gpu_lib.find_status(img, out=np.zeros(cap, np.uint64))
+        assert status == -1
+    finally:
+        buf.close()
