@@ -70,6 +70,7 @@ struct LabArgs {
   uint32_t *comp_root, *msize, *members;
   uint64_t *mpk;
   uint64_t *runs; // per batch: lab_link's entries, see lab_gather
+  uint32_t *run_starts; // bit p & 31 of word p >> 5: position p starts a run
   Spot *spot_tmp;
   Pixel *pix_tmp;
   uint64_t *pack;
@@ -105,12 +106,15 @@ __device__ __forceinline__ uint32_t uf_find(uint32_t *parent, uint32_t x) {
   }
 }
 
-__device__ __forceinline__ void uf_unite(uint32_t *parent, uint32_t a, uint32_t b) {
+// Joins the trees of a and b; returns the merged tree's root as it was at
+// the link (an ancestor of both from then on), so a caller uniting one
+// element with several others can pass it back as `a`.
+__device__ __forceinline__ uint32_t uf_unite(uint32_t *parent, uint32_t a, uint32_t b) {
   while (true) {
     a = uf_find(parent, a);
     b = uf_find(parent, b);
     if (a == b)
-      return;
+      return a;
     if (a < b) {
       const uint32_t t = a;
       a = b;
@@ -119,7 +123,7 @@ __device__ __forceinline__ void uf_unite(uint32_t *parent, uint32_t a, uint32_t 
     // Link the higher root under the lower one, if it is still a root.
     const uint32_t old = atomicCAS(&parent[a], a, b);
     if (old == a)
-      return;
+      return b;
     a = old;
   }
 }
@@ -261,9 +265,15 @@ __global__ void __launch_bounds__(kThreads) lab_gather(LabArgs a) {
         const uint64_t b0 = i == 0 ? 0 : (prev >> kBlockShift) + 1;
         for (uint64_t b = b0; b <= b1; b++)
           tab[b] = static_cast<uint32_t>(i);
+      } else if (g > sc->carry_last_start) {
+        // the carried last frame, which the first batch frame links to
+        const uint32_t v = a.ix[g];
+        left = v % W != 0 && a.ix[g - 1] + 1 == v;
       }
     }
     const uint32_t linked = __ballot_sync(kFull, left);
+    if (lane == 0 && base < n)
+      a.run_starts[base >> 5] = ~linked;
     const bool mine = g < n && g >= carry;
     if (mine) {
       // the run's first lane in this chunk: the highest lane at or below
@@ -314,22 +324,39 @@ __device__ __forceinline__ uint64_t first_at_least(const LabArgs &a, const uint3
   return q;
 }
 
-// Unites the run whose first pixel is g with every run of the list at s0
-// that has a pixel with an index in [lo, hi] (one row's span).
-__device__ __forceinline__ void unite_overlaps(const LabArgs &a, uint32_t g, const uint32_t *tab,
-                                               uint64_t s0, uint64_t count, uint32_t lo,
-                                               uint32_t hi) {
-  uint32_t prev = 0;
-  bool first = true;
-  for (uint64_t q = first_at_least(a, tab, s0, count, lo); q < count; q++) {
-    const uint32_t v = a.ix[s0 + q];
-    if (v > hi)
+// Unites the tree of `ra` (the run whose first pixel is g, or an ancestor)
+// with every run of the list at s0 that has a pixel with an index in
+// [lo, hi] (one row's span, at most 32 indices): the run holding the first
+// such pixel, then the later run starts, found in the run-start bitmap;
+// returns the merged root.
+__device__ __forceinline__ uint32_t unite_overlaps(const LabArgs &a, uint32_t ra,
+                                                   const uint32_t *tab, uint64_t s0,
+                                                   uint64_t count, uint32_t lo, uint32_t hi) {
+  const uint64_t q = first_at_least(a, tab, s0, count, lo);
+  if (q >= count)
+    return ra;
+  uint64_t p = s0 + q;
+  const uint64_t end = s0 + count;
+  if (a.ix[p] > hi)
+    return ra;
+  ra = uf_unite(a.par, ra, static_cast<uint32_t>(p));
+  for (p++; p < end;) {
+    const uint32_t w = a.run_starts[p >> 5] & (0xffffffffu << (p & 31));
+    if (!w) {
+      // the rest of the chunk continues the run; the next start is after it
+      const uint64_t lastp = p | 31;
+      if (lastp + 1 >= end || a.ix[lastp] >= hi)
+        break;
+      p = lastp + 1;
+      continue;
+    }
+    p = (p & ~31ull) + static_cast<uint64_t>(__ffs(w) - 1);
+    if (p >= end || a.ix[p] > hi)
       break;
-    if (first || v != prev + 1) // the first pixel of a run within the span
-      uf_unite(a.par, g, static_cast<uint32_t>(s0 + q));
-    first = false;
-    prev = v;
+    ra = uf_unite(a.par, ra, static_cast<uint32_t>(p));
+    p++;
   }
+  return ra;
 }
 
 // The links of src/dials_spots.cc:106-137 -- left, up, and the same pixel on
@@ -341,21 +368,20 @@ __device__ __forceinline__ void unite_overlaps(const LabArgs &a, uint32_t g, con
 // up or previous-frame edge of the run's pixels ends in one of those runs.
 __global__ void __launch_bounds__(kThreads) lab_link(LabArgs a) {
   const LabelScalars *sc = a.sc;
-  const uint64_t n = sc->n, carry = sc->carry_n;
+  const uint64_t carry = sc->carry_n;
   const int first_batch_seg = carry > 0 ? 1 : 0;
   const uint32_t W = static_cast<uint32_t>(a.width);
   const int64_t z0 = sc->batch_z0;
   const uint32_t nruns = sc->runs_n;
-  (void)n;
-  (void)carry;
   // one entry of lab_gather's list per thread, so the lanes of a warp all
   // have a run to link
   for (uint64_t i = gtid(); i < nruns; i += gstride()) {
     const uint64_t e = a.runs[i];
     const uint64_t g = e & 0xffffffffu;
     const uint32_t len = static_cast<uint32_t>(e >> 32) & 0x3fu;
+    uint32_t ra = static_cast<uint32_t>(g);
     if (e >> 40) // a run crossing into a new chunk: join the pieces
-      uf_unite(a.par, static_cast<uint32_t>(g), static_cast<uint32_t>(g - 1));
+      ra = uf_unite(a.par, ra, static_cast<uint32_t>(g - 1));
     // the batch's frames are consecutive: a new pixel's frame is its segment
     const int s = first_batch_seg + static_cast<int>(a.fr[g] - z0);
     const uint64_t s0 = a.seg_start[s];
@@ -363,11 +389,11 @@ __global__ void __launch_bounds__(kThreads) lab_link(LabArgs a) {
     const uint32_t idx = a.ix[g];
     const uint32_t last = idx + len - 1; // the piece's last index (one row, one chunk)
     if (idx >= W)
-      unite_overlaps(a, static_cast<uint32_t>(g), table_of(a, s, first_batch_seg), s0, end - s0,
-                     idx - W, last - W);
+      ra = unite_overlaps(a, ra, table_of(a, s, first_batch_seg), s0, end - s0, idx - W,
+                          last - W);
     if (!a.two_d && s > 0 && a.seg_z[s - 1] + 1 == a.seg_z[s])
-      unite_overlaps(a, static_cast<uint32_t>(g), table_of(a, s - 1, first_batch_seg),
-                     a.seg_start[s - 1], a.seg_count[s - 1], idx, last);
+      unite_overlaps(a, ra, table_of(a, s - 1, first_batch_seg), a.seg_start[s - 1],
+                     a.seg_count[s - 1], idx, last);
   }
 }
 
@@ -1146,7 +1172,7 @@ void DeviceLabeller::release() {
     l = Live();
   }
   void *ptrs[] = {root_, size_, rank_of_root_, cursor_, lastz_, bits_, bcnt_, comp_root_,
-                  msize_, mpk_, runs_, spot_tmp_, pix_tmp_, members_, pack_, open_, spots_out_, kept_out_, seg_start_,
+                  msize_, mpk_, runs_, run_starts_, spot_tmp_, pix_tmp_, members_, pack_, open_, spots_out_, kept_out_, seg_start_,
                   seg_count_, seg_z_, tab_};
   for (void *p : ptrs)
     cudaFree(p);
@@ -1156,6 +1182,7 @@ void DeviceLabeller::release() {
   bits_ = bcnt_ = comp_root_ = msize_ = members_ = open_ = nullptr;
   mpk_ = pack_ = nullptr;
   runs_ = nullptr;
+  run_starts_ = nullptr;
   spot_tmp_ = nullptr;
   pix_tmp_ = nullptr;
   spots_out_ = nullptr;
@@ -1211,6 +1238,7 @@ void DeviceLabeller::reserve(uint64_t batch_pixels, int max_frames, uint64_t car
     alloc(&msize_, live, "member sizes");
     alloc(&mpk_, live, "member offsets");
     alloc(&runs_, live, "run list");
+    alloc(&run_starts_, live / 32 + 1, "run starts");
     alloc(&members_, live, "members");
     alloc(&pack_, live, "spot offsets");
     alloc(&open_, live, "open flags");
@@ -1296,6 +1324,7 @@ void DeviceLabeller::enqueue(int nframes, const SignalPixel *lists, const uint64
   a.msize = msize_;
   a.mpk = mpk_;
   a.runs = runs_;
+  a.run_starts = run_starts_;
   a.spot_tmp = spot_tmp_;
   a.pix_tmp = pix_tmp_;
   a.members = members_;
