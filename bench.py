@@ -418,9 +418,10 @@ def run_ours(args, ranks):
                          "and 3D grouping on one, as the reference CLI runs them"}
 
     # threshold; placement reduce, scan, copy; grouping: setup, gather, link,
-    # keep_table, flatten, mark, rank, scatter, accept (small and large
-    # components), write, open, carry, finalize, and 4 scans of 3 launches
-    launches_per_step = 1 + 3 + (14 + 4 * 3)
+    # keep_table, flatten, mark, compact, count, rank, scatter, accept (small
+    # and large components), write, open, carry, finalize, and 5 scans of 3
+    # launches
+    launches_per_step = 1 + 3 + (16 + 5 * 3)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ranks.world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,

@@ -15,9 +15,13 @@
 //             union-find that links toward the lower position, so a root is
 //             its component's first pixel in (frame, index) order
 //   flatten   root of every pixel; component size and last frame
-//   mark      finished roots (no pixel on the batch's last frame) as one
-//             bitmap per last-frame bucket, with per-word counts
-//   scan      of the counts, bucket-major: the reference's emission order
+//   mark      finished roots (no pixel on the batch's last frame) as a
+//             bitmap, with a count per 32-position word
+//   scan      of the counts
+//   compact   the finished roots, in position order
+//   count     per 32 roots of that list, how many close on each frame
+//             (last-frame bucket)
+//   scan      of those counts, bucket-major: the reference's emission order
 //             is (last frame, first pixel), which is exactly bucket then
 //             position
 //   rank      each finished component's emission rank; size filters
@@ -66,7 +70,8 @@ struct LabArgs {
   uint32_t *root, *size;
   int32_t *lastz;
   uint32_t *rank_of_root, *cursor;
-  uint32_t *bits, *bcnt;
+  uint32_t *bits, *bcnt; // finished-root bitmap; word counts, then bucket counts
+  uint32_t *flist;       // the finished roots in position order
   uint32_t *comp_root, *msize, *members;
   uint64_t *mpk;
   uint64_t *runs; // per batch: lab_link's entries, see lab_gather
@@ -203,7 +208,6 @@ __global__ void lab_setup(LabArgs a) {
   sc->n = pos;
   sc->nw = (pos + 31) / 32;
   sc->nseg = nseg;
-  sc->seg_len = static_cast<uint64_t>(nseg) * sc->nw;
   sc->signal_pixels += pos - carry;
   sc->closed32 = sc->open32 = 0;
   sc->runs_n = 0;
@@ -436,39 +440,77 @@ __global__ void __launch_bounds__(kThreads) lab_flatten(LabArgs a) {
 __global__ void __launch_bounds__(kThreads) lab_mark(LabArgs a) {
   const LabelScalars *sc = a.sc;
   const uint64_t n = sc->n, nw = sc->nw;
-  const int nseg = static_cast<int>(sc->nseg);
   const int lane = threadIdx.x & 31;
   const uint64_t warp = gtid() >> 5, nwarps = gstride() >> 5;
   for (uint64_t w = warp; w < nw; w += nwarps) {
-    const uint64_t g = w * 32 + lane;
-    const bool fin = finished_root(a, g, n);
-    const int b = fin ? bucket_of(a.seg_z, nseg, a.lastz[g]) : -1;
+    const uint32_t m = __ballot_sync(kFull, finished_root(a, w * 32 + lane, n));
+    if (lane == 0) {
+      a.bits[w] = m;
+      a.bcnt[w] = __popc(m);
+    }
+  }
+}
+
+// The finished roots in position order, from the bitmap and the scanned
+// word counts (a thread per word: most words hold none, few more than one).
+// Also the length of the bucket-count table that the next scan covers.
+__global__ void __launch_bounds__(kThreads) lab_compact(LabArgs a) {
+  LabelScalars *sc = a.sc;
+  const uint64_t nw = sc->nw;
+  if (gtid() == 0) {
+    const uint64_t closed = sc->closed32;
+    sc->closed = closed;
+    sc->seg_len = sc->nseg * ((closed + 31) / 32);
+  }
+  for (uint64_t w = gtid(); w < nw; w += gstride()) {
+    uint32_t m = a.bits[w];
+    uint32_t at = a.bcnt[w];
+    while (m) {
+      a.flist[at++] = static_cast<uint32_t>(w * 32 + __ffs(m) - 1);
+      m &= m - 1;
+    }
+  }
+}
+
+// Per 32 consecutive roots of the list, how many close in each bucket, laid
+// out bucket-major (bucket s, group j at s * groups + j).
+__global__ void __launch_bounds__(kThreads) lab_count(LabArgs a) {
+  const LabelScalars *sc = a.sc;
+  const uint64_t closed = sc->closed, groups = (closed + 31) / 32;
+  const int nseg = static_cast<int>(sc->nseg);
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = gtid() >> 5, nwarps = gstride() >> 5;
+  for (uint64_t j = warp; j < groups; j += nwarps) {
+    const uint64_t k = j * 32 + lane;
+    const int b = k < closed ? bucket_of(a.seg_z, nseg, a.lastz[a.flist[k]]) : -1;
     for (int s = 0; s < nseg; s++) {
       const uint32_t m = __ballot_sync(kFull, b == s);
-      if (lane == 0) {
-        a.bits[s * nw + w] = m;
-        a.bcnt[s * nw + w] = __popc(m);
-      }
+      if (lane == 0)
+        a.bcnt[s * groups + j] = __popc(m);
     }
   }
 }
 
 __global__ void __launch_bounds__(kThreads) lab_rank(LabArgs a) {
   LabelScalars *sc = a.sc;
-  const uint64_t n = sc->n, nw = sc->nw;
+  const uint64_t closed = sc->closed, groups = (closed + 31) / 32;
   const int nseg = static_cast<int>(sc->nseg);
-  if (gtid() == 0)
-    sc->closed = sc->closed32;
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = gtid() >> 5, nwarps = gstride() >> 5;
   uint32_t small = 0, large = 0;
-  for (uint64_t g = gtid(); g < n; g += gstride()) {
-    if (!finished_root(a, g, n))
+  for (uint64_t j = warp; j < groups; j += nwarps) {
+    const uint64_t k = j * 32 + lane;
+    const bool valid = k < closed;
+    const uint32_t g = valid ? a.flist[k] : 0u;
+    const int b = valid ? bucket_of(a.seg_z, nseg, a.lastz[g]) : -1;
+    // earlier roots of this group in the same bucket come first
+    const uint32_t peers = __match_any_sync(kFull, b);
+    if (!valid)
       continue;
-    const int b = bucket_of(a.seg_z, nseg, a.lastz[g]);
-    const uint64_t w = g >> 5;
-    const uint32_t lane_mask = (1u << (g & 31)) - 1u;
-    const uint32_t rank = a.bcnt[b * nw + w] + __popc(a.bits[b * nw + w] & lane_mask);
+    const uint32_t rank =
+        a.bcnt[b * groups + j] + __popc(peers & ((1u << lane) - 1u));
     a.rank_of_root[g] = rank;
-    a.comp_root[rank] = static_cast<uint32_t>(g);
+    a.comp_root[rank] = g;
     const uint32_t size = a.size[g];
     const bool keep = size >= a.min_size && size <= a.max_size;
     a.msize[rank] = keep ? size : 0u;
@@ -1171,7 +1213,7 @@ void DeviceLabeller::release() {
     cudaFree(l.parent);
     l = Live();
   }
-  void *ptrs[] = {root_, size_, rank_of_root_, cursor_, lastz_, bits_, bcnt_, comp_root_,
+  void *ptrs[] = {root_, size_, rank_of_root_, cursor_, lastz_, bits_, bcnt_, flist_, comp_root_,
                   msize_, mpk_, runs_, run_starts_, spot_tmp_, pix_tmp_, members_, pack_, open_, spots_out_, kept_out_, seg_start_,
                   seg_count_, seg_z_, tab_};
   for (void *p : ptrs)
@@ -1179,7 +1221,7 @@ void DeviceLabeller::release() {
   tab_ = nullptr;
   root_ = size_ = rank_of_root_ = cursor_ = nullptr;
   lastz_ = nullptr;
-  bits_ = bcnt_ = comp_root_ = msize_ = members_ = open_ = nullptr;
+  bits_ = bcnt_ = flist_ = comp_root_ = msize_ = members_ = open_ = nullptr;
   mpk_ = pack_ = nullptr;
   runs_ = nullptr;
   run_starts_ = nullptr;
@@ -1232,8 +1274,9 @@ void DeviceLabeller::reserve(uint64_t batch_pixels, int max_frames, uint64_t car
     alloc(&rank_of_root_, live, "ranks");
     alloc(&cursor_, live, "cursors");
     alloc(&lastz_, live, "last frames");
-    alloc(&bits_, (fc + 1) * nwmax, "bucket bitmaps");
+    alloc(&bits_, nwmax, "finished-root bitmap");
     alloc(&bcnt_, (fc + 1) * nwmax, "bucket counts");
+    alloc(&flist_, live, "finished roots");
     alloc(&comp_root_, live, "components");
     alloc(&msize_, live, "member sizes");
     alloc(&mpk_, live, "member offsets");
@@ -1320,6 +1363,7 @@ void DeviceLabeller::enqueue(int nframes, const SignalPixel *lists, const uint64
   a.cursor = cursor_;
   a.bits = bits_;
   a.bcnt = bcnt_;
+  a.flist = flist_;
   a.comp_root = comp_root_;
   a.msize = msize_;
   a.mpk = mpk_;
@@ -1352,8 +1396,11 @@ void DeviceLabeller::enqueue(int nframes, const SignalPixel *lists, const uint64
   lab_flatten<<<grid, kThreads, 0, s>>>(a);
   lab_mark<<<grid, kThreads, 0, s>>>(a);
   const uint64_t nwmax = live_cap_ / 32 + 1;
+  scan32_.run(bcnt_, bcnt_, &sc->nw, 1, nwmax, &sc->closed32, s);
+  lab_compact<<<grid, kThreads, 0, s>>>(a);
+  lab_count<<<grid, kThreads, 0, s>>>(a);
   scan32_.run(bcnt_, bcnt_, &sc->seg_len, 1, static_cast<uint64_t>(frame_cap_ + 1) * nwmax,
-              &sc->closed32, s);
+              nullptr, s);
   lab_rank<<<grid, kThreads, 0, s>>>(a);
   scan64_.run(mpk_, mpk_, &sc->closed, 1, live_cap_, &sc->members_pack, s);
   lab_scatter<<<grid, kThreads, 0, s>>>(a);

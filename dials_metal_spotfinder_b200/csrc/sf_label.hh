@@ -47,7 +47,7 @@ struct LabelScalars {
   uint64_t n;             // live pixels (carried + new)
   uint64_t nw;            // 32-pixel words over n
   uint64_t nseg;          // frame segments (carried last frame + batch frames)
-  uint64_t seg_len;       // nseg * nw
+  uint64_t seg_len;       // bucket-count table length: nseg * ceil(closed / 32)
   uint64_t closed;        // finished components
   uint32_t closed32, open32;
   uint32_t runs_n, pad0;  // lab_link's work list
@@ -128,7 +128,8 @@ private:
   } live_[2];
   uint32_t *root_ = nullptr, *size_ = nullptr, *rank_of_root_ = nullptr, *cursor_ = nullptr;
   int32_t *lastz_ = nullptr;
-  uint32_t *bits_ = nullptr, *bcnt_ = nullptr; // bucket bitmaps and their word counts
+  uint32_t *bits_ = nullptr, *bcnt_ = nullptr; // finished-root bitmap; counts (see lab_mark)
+  uint32_t *flist_ = nullptr;                   // the finished roots in position order
   uint32_t *comp_root_ = nullptr, *msize_ = nullptr, *members_ = nullptr;
   uint64_t *mpk_ = nullptr; // member offset (low 32) | size-filtered index (high 32)
   uint64_t *runs_ = nullptr; // lab_link's work list
