@@ -422,6 +422,11 @@ def run_ours(args, ranks):
     # and large components), write, open, carry, finalize, and 5 scans of 3
     # launches
     launches_per_step = 1 + 3 + (16 + 5 * 3)
+    # the whole pipeline's algorithmic bytes per frame: one read of the
+    # frame, the signal list written and read back by the grouping, the
+    # spot rows written
+    sig_per_frame = statistics.mean(nsig_per_step) / F
+    pipe_bytes = frame_bytes + 32 * sig_per_frame + 104 * spots_per_frame
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ranks.world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
@@ -446,7 +451,13 @@ def run_ours(args, ranks):
         "stage_ms_per_step": {"threshold": thr_ms,
                               "placement": stage["place_ms"] / max(stage["runs"], 1),
                               "grouping": stage["group_ms"] / max(stage["runs"], 1)},
-        "signal_pixels_per_frame": statistics.mean(nsig_per_step) / F,
+        "signal_pixels_per_frame": sig_per_frame,
+        "gpixels_per_s": value * SHAPE[0] * SHAPE[1] / 1e9,
+        "pipeline_bytes": {"per_frame": pipe_bytes,
+                           "achieved_gbs": value * pipe_bytes / 1e9,
+                           "frac": value * pipe_bytes / 1e9 / peak, "peak_kind": peak_kind,
+                           "counted": "frame read + 32 B per signal pixel (list written, "
+                                      "read by the grouping) + 104 B per spot row"},
         "clocks": clocks.summary(),
         "gpu_launches": launches_per_step * args.steps,
         "e2e": e2e,
