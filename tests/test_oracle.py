@@ -104,6 +104,39 @@ def test_oracle_grouping_equals_reference_with_gaps_and_long_streaks():
             assert a.counts == b.counts
 
 
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built here")
+@pytest.mark.parametrize("config", ["4m_u16", "16m_u32"])
+def test_oracle_equals_reference_on_detector_frames(config):
+    """Whole detector frames at the benchmark's density (module gaps,
+    Poisson ring, reflections): the restatement and the reference's own
+    dext<T> give the same list, byte for byte."""
+    from dials_metal_spotfinder_b200 import synth
+    if config == "4m_u16":
+        img = synth.eiger_4m(frames=2).frame(1)
+    else:
+        img = synth.eiger_16m(frames=2, dtype=np.uint32).frame(1)
+    a = O.dext(img, use_ref=True)
+    b = O.dext(img)
+    assert a[0] == b[0] == 0 and a[2] == b[2] > 1000
+    assert a[1].tobytes() == b[1].tobytes()
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built here")
+def test_oracle_grouping_equals_reference_on_a_4m_series():
+    """Eight consecutive 4M frames, thresholded by the reference, grouped in
+    3D and in 2D with the default options by both."""
+    from dials_metal_spotfinder_b200 import synth
+    series = synth.eiger_4m(frames=8)
+    frames = [series.frame(z) for z in range(8)]
+    sigs = [O.dext(img, use_ref=True)[1] for img in frames]
+    for two_d in (False, True):
+        a = O.group(sigs, *frames[0].shape, use_ref=True, two_d=two_d)
+        b = O.group(sigs, *frames[0].shape, two_d=two_d)
+        assert a.counts == b.counts and a.counts["accepted"] > 100
+        assert a.spots.tobytes() == b.spots.tobytes()
+        assert a.pixels.tobytes() == b.pixels.tobytes()
+
+
 # -- hand-derived cases from the reference's tests/test_dials_spots.cc -------
 
 H, W = 8, 10
