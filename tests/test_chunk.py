@@ -141,6 +141,29 @@ def test_liblz4_blocks_decode_with_ours():
     assert np.array_equal(back, img)
 
 
+@needs_liblz4
+@pytest.mark.parametrize("block", [65536, 1 << 30])
+def test_large_lz4_blocks_decode_on_the_host(block):
+    """HDF5's LZ4 filter writes blocks far beyond 8 KB (1 GB by default, so a
+    frame is one block): liblz4's blocks of 64 KB and of the whole frame
+    decode to the frame, and a block cut short is refused."""
+    rng = np.random.default_rng(12)
+    img = rng.poisson(0.9, (333, 517)).astype(np.uint16)
+    img[::11, ::3] = 4000
+    raw = img.reshape(-1).view(np.uint8).tobytes()
+    out = bytearray(struct.pack(">QI", len(raw), block))
+    for at in range(0, len(raw), block):
+        src = raw[at:at + block]
+        dst = ctypes.create_string_buffer(len(src) + len(src) // 255 + 64)
+        cs = LZ4.LZ4_compress_default(src, dst, len(src), len(dst))
+        assert cs > 0
+        out += struct.pack(">I", cs) + dst.raw[:cs]
+    good = np.frombuffer(bytes(out), np.uint8)
+    assert np.array_equal(C.decode(good, img.shape, np.uint16, "lz4"), img)
+    with pytest.raises(BadArgument):
+        C.decode(good[:-1], img.shape, np.uint16, "lz4")
+
+
 def test_malformed_chunks_are_refused():
     rng = np.random.default_rng(2)
     img = rng.poisson(2.0, (100, 90)).astype(np.uint16)
