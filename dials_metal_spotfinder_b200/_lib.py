@@ -110,6 +110,7 @@ SIGNATURES = {
     "sf_engine_upload": (_I, [_P, _I, _I, _P]),
     "sf_engine_upload_device": (_I, [_P, _I, _I, _P, _S]),
     "sf_engine_upload_chunk": (_I, [_P, _I, _I, _P, _S, _I]),
+    "sf_engine_upload_chunks": (_I, [_P, _I, _S, _P, _P, _P, _I]),
     "sf_engine_set_pixel_mask": (_I, [_P, _I, _P]),
     "sf_engine_run": (_I, [_P, _I]),
     "sf_engine_use_graph": (_I, [_P, _I]),

@@ -134,6 +134,20 @@ int sf_engine_upload_chunk(sf_engine *engine, int slot, int frame, const void *c
   });
 }
 
+int sf_engine_upload_chunks(sf_engine *engine, int slot, size_t count, const int *frames,
+                            const void *const *chunks, const size_t *nbytes, int algorithm) {
+  return guarded([&] {
+    if (!engine || (count && (!chunks || !nbytes)))
+      return -1;
+    for (size_t k = 0; k < count; k++)
+      if (!chunks[k])
+        return -1;
+    reinterpret_cast<Engine *>(engine)->upload_chunks(slot, count, frames, chunks, nbytes,
+                                                      algorithm);
+    return 0;
+  });
+}
+
 int sf_engine_set_pixel_mask(sf_engine *engine, int frame, const uint8_t *mask) {
   return guarded([&] {
     if (!engine)

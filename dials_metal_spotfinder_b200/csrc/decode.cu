@@ -567,13 +567,19 @@ DeviceChunkDecoder::~DeviceChunkDecoder() {
     cudaStreamSynchronize(h2d_);
   for (Set &S : sets_) {
     cudaFree(S.d_in);
-    cudaFree(S.d_table);
-    if (S.h_table)
-      cudaFreeHost(S.h_table);
     if (S.copied)
       cudaEventDestroy(S.copied);
     if (S.freed)
       cudaEventDestroy(S.freed);
+  }
+  for (Table &T : tables_) {
+    cudaFree(T.d);
+    if (T.h)
+      cudaFreeHost(T.h);
+    if (T.copied)
+      cudaEventDestroy(T.copied);
+    if (T.freed)
+      cudaEventDestroy(T.freed);
   }
   if (h2d_)
     cudaStreamDestroy(h2d_);
@@ -597,31 +603,21 @@ void DeviceChunkDecoder::prepare() {
     check(cudaEventCreateWithFlags(&S.copied, cudaEventDisableTiming), "cudaEventCreate");
     check(cudaEventCreateWithFlags(&S.freed, cudaEventDisableTiming), "cudaEventCreate");
   }
+  for (Table &T : tables_) {
+    check(cudaEventCreateWithFlags(&T.copied, cudaEventDisableTiming), "cudaEventCreate");
+    check(cudaEventCreateWithFlags(&T.freed, cudaEventDisableTiming), "cudaEventCreate");
+  }
   check(cudaStreamCreateWithFlags(&h2d_, cudaStreamNonBlocking), "cudaStreamCreate");
 }
 
-DeviceChunkDecoder::Set &DeviceChunkDecoder::next_set(size_t in_bytes, size_t entries) {
+DeviceChunkDecoder::Set &DeviceChunkDecoder::next_set(size_t in_bytes) {
   prepare();
   Set &S = sets_[next_];
   next_ = (next_ + 1) % kSets;
-  if (S.used)
-    // the host rewrites the set's page-locked table below
-    check(cudaEventSynchronize(S.copied), "waiting for a staging set");
-  if (in_bytes > S.in_cap || entries > S.table_cap) {
+  if (in_bytes > S.in_cap) {
     if (S.used)
       check(cudaEventSynchronize(S.freed), "waiting for a staging set");
     grow(&S.d_in, S.in_cap, in_bytes, "cudaMalloc chunk staging");
-    if (entries > S.table_cap) {
-      if (S.h_table)
-        cudaFreeHost(S.h_table);
-      S.h_table = nullptr;
-      cudaFree(S.d_table);
-      S.d_table = nullptr;
-      S.table_cap = 0;
-      check(cudaMallocHost(&S.h_table, entries * sizeof(BlockDesc)), "cudaMallocHost block table");
-      check(cudaMalloc(&S.d_table, entries * sizeof(BlockDesc)), "cudaMalloc block table");
-      S.table_cap = entries;
-    }
   }
   // the copy may overwrite the set once the decode that read it is done
   check(cudaStreamWaitEvent(h2d_, S.freed, 0), "ordering a staging set");
@@ -629,9 +625,36 @@ DeviceChunkDecoder::Set &DeviceChunkDecoder::next_set(size_t in_bytes, size_t en
   return S;
 }
 
+DeviceChunkDecoder::Table &DeviceChunkDecoder::next_table(size_t entries) {
+  prepare();
+  Table &T = tables_[next_table_];
+  next_table_ = (next_table_ + 1) % kTables;
+  if (T.used)
+    // the host rewrites the page-locked copy below
+    check(cudaEventSynchronize(T.copied), "waiting for a block table");
+  if (entries > T.cap) {
+    if (T.used)
+      check(cudaEventSynchronize(T.freed), "waiting for a block table");
+    if (T.h)
+      cudaFreeHost(T.h);
+    T.h = nullptr;
+    cudaFree(T.d);
+    T.d = nullptr;
+    T.cap = 0;
+    check(cudaMallocHost(&T.h, entries * sizeof(BlockDesc)), "cudaMallocHost block table");
+    check(cudaMalloc(&T.d, entries * sizeof(BlockDesc)), "cudaMalloc block table");
+    T.cap = entries;
+  }
+  check(cudaStreamWaitEvent(h2d_, T.freed, 0), "ordering a block table");
+  T.used = true;
+  return T;
+}
+
 void DeviceChunkDecoder::reserve(size_t chunk_bytes, size_t blocks) {
   for (int k = 0; k < kSets; k++)
-    next_set(round16(chunk_bytes) + 16, std::max<size_t>(blocks, 1));
+    next_set(round16(chunk_bytes) + 16);
+  for (int k = 0; k < kTables; k++)
+    next_table(std::max<size_t>(blocks, 1));
 }
 
 void DeviceChunkDecoder::enqueue_raw(const void *src, size_t height, size_t row_bytes, void *dst,
@@ -639,7 +662,7 @@ void DeviceChunkDecoder::enqueue_raw(const void *src, size_t height, size_t row_
   const size_t bytes = height * row_bytes;
   if (bytes == 0)
     return;
-  Set &S = next_set(round16(bytes), 1);
+  Set &S = next_set(round16(bytes));
   check(cudaMemcpyAsync(S.d_in, src, bytes, cudaMemcpyDefault, h2d_), "copying a frame");
   check(cudaEventRecord(S.copied, h2d_), "cudaEventRecord");
   check(cudaStreamWaitEvent(s, S.copied, 0), "ordering after the copy");
@@ -661,8 +684,9 @@ void DeviceChunkDecoder::enqueue(const uint8_t *chunk, size_t nbytes, const Chun
   const size_t nb = L.block_in.size();
   if (nb == 0 && L.raw_bytes == 0)
     return;
-  Set &S = next_set(round16(nbytes) + 16, std::max<size_t>(nb, 1));
-  BlockDesc *t = static_cast<BlockDesc *>(S.h_table);
+  Set &S = next_set(round16(nbytes) + 16);
+  Table &T = next_table(std::max<size_t>(nb, 1));
+  BlockDesc *t = static_cast<BlockDesc *>(T.h);
   uint32_t max_len = 0;
   for (size_t b = 0; b < nb; b++) {
     t[b] = BlockDesc{L.block_in[b], L.block_out[b], L.block_len[b], L.block_n[b]};
@@ -670,14 +694,14 @@ void DeviceChunkDecoder::enqueue(const uint8_t *chunk, size_t nbytes, const Chun
   }
   check(cudaMemcpyAsync(S.d_in, chunk, nbytes, cudaMemcpyDefault, h2d_), "copying a chunk");
   if (nb)
-    check(cudaMemcpyAsync(S.d_table, S.h_table, nb * sizeof(BlockDesc), cudaMemcpyHostToDevice,
-                          h2d_),
+    check(cudaMemcpyAsync(T.d, T.h, nb * sizeof(BlockDesc), cudaMemcpyHostToDevice, h2d_),
           "copying a block table");
   check(cudaEventRecord(S.copied, h2d_), "cudaEventRecord");
+  check(cudaEventRecord(T.copied, h2d_), "cudaEventRecord");
   check(cudaStreamWaitEvent(s, S.copied, 0), "ordering after the copy");
 
   const uint64_t frame_bytes = static_cast<uint64_t>(height) * row_bytes;
-  const auto *tbl = static_cast<const BlockDesc *>(S.d_table);
+  const auto *tbl = static_cast<const BlockDesc *>(T.d);
   const uint32_t n32 = static_cast<uint32_t>(nb);
   if (L.block_bytes > kMaxBlockBytes) {
     // plain LZ4 with blocks beyond shared memory (bitshuffle blocks never
@@ -690,6 +714,7 @@ void DeviceChunkDecoder::enqueue(const uint8_t *chunk, size_t nbytes, const Chun
     check(cudaGetLastError(), "launching the chunk decoder");
     repitch(d_linear_, height, row_bytes, dst, dst_pitch, s);
     check(cudaEventRecord(S.freed, s), "cudaEventRecord");
+    check(cudaEventRecord(T.freed, s), "cudaEventRecord");
     return;
   }
   const uint32_t out_bytes = static_cast<uint32_t>(round16(std::max<uint64_t>(L.block_bytes, 16)));
@@ -721,6 +746,7 @@ void DeviceChunkDecoder::enqueue(const uint8_t *chunk, size_t nbytes, const Chun
                                                            raw_out, d_err_);
   check(cudaGetLastError(), "launching the chunk decoder");
   check(cudaEventRecord(S.freed, s), "cudaEventRecord");
+  check(cudaEventRecord(T.freed, s), "cudaEventRecord");
 }
 
 int *DeviceChunkDecoder::error_flag() {

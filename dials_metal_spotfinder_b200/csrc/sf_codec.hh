@@ -71,24 +71,36 @@ public:
   // cleared on first use.
   int *error_flag();
 
-  static constexpr int kSets = 3;
+  static constexpr int kSets = 3;    // device staging buffers for chunks
+  static constexpr int kTables = 32; // block tables, so the host rarely waits
 
 private:
+  // A chunk's (or raw frame's) bytes on the device. Ordered on the device
+  // only: the copy into it waits for the decode that last read it.
   struct Set {
-    uint8_t *d_in = nullptr; // the chunk (or raw frame) on the device
+    uint8_t *d_in = nullptr;
     size_t in_cap = 0;
-    void *h_table = nullptr; // block table, page-locked, and its device copy
-    void *d_table = nullptr;
-    size_t table_cap = 0;    // entries
-    cudaEvent_t copied = nullptr; // the set's host-to-device copies are done
-    cudaEvent_t freed = nullptr;  // the decode that read the set is done
+    cudaEvent_t copied = nullptr; // its host-to-device copies are done
+    cudaEvent_t freed = nullptr;  // the decode that read it is done
     bool used = false;
   };
-  Set &next_set(size_t in_bytes, size_t entries);
+  // A block table, page-locked for the copy and on the device. The host
+  // rewrites one only after its copy of kTables uploads ago is done.
+  struct Table {
+    void *h = nullptr;
+    void *d = nullptr;
+    size_t cap = 0; // entries
+    cudaEvent_t copied = nullptr;
+    cudaEvent_t freed = nullptr;
+    bool used = false;
+  };
+  Set &next_set(size_t in_bytes);
+  Table &next_table(size_t entries);
   void prepare();
 
   Set sets_[kSets];
-  int next_ = 0;
+  Table tables_[kTables];
+  int next_ = 0, next_table_ = 0;
   cudaStream_t h2d_ = nullptr;
   uint8_t *d_linear_ = nullptr; // a frame decoded from blocks beyond shared memory
   size_t linear_cap_ = 0;

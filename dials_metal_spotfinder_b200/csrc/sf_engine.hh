@@ -11,6 +11,7 @@
 #include "sf_codec.hh"
 #include "sf_host.hh"
 #include "sf_label.hh"
+#include "sf_pool.hh"
 
 namespace sf {
 
@@ -59,6 +60,9 @@ struct Engine {
   LabelScalars *host_sc = nullptr;
   // Compressed uploads, decoded on the device in the copy stream.
   DeviceChunkDecoder decoder;
+  // Host threads for the framing walks of a batch of chunks, made on first
+  // use.
+  std::unique_ptr<HostPool> pool;
   // Host callbacks in the run's stream, captured into its graphs too: after
   // the signal lists are placed and after the grouping, each given its
   // slot's argument. Set them before the first run.
@@ -397,6 +401,41 @@ struct Engine {
       mask_n = all.size();
     }
     drop_graphs();
+  }
+
+  // Several chunks at once: their framing is walked on host threads in
+  // parallel (each walk is a chain of dependent loads through its chunk),
+  // all checked before anything is enqueued, then the copies and decodes go
+  // in order as upload_chunk's would.
+  void upload_chunks(int slot, size_t n, const int *frames, const void *const *chunks,
+                     const size_t *nbytes, int algorithm) {
+    check_slot(slot);
+    for (size_t k = 0; k < n; k++)
+      check_frame(frames ? frames[k] : static_cast<int>(k));
+    const size_t eb = static_cast<size_t>(plan->elem_bytes());
+    std::vector<ChunkLayout> layouts(n);
+    auto frame_of = [&](size_t k) { return frames ? frames[k] : static_cast<int>(k); };
+    auto parse = [&](size_t k) {
+      const ThresholdPlan::Shape &sh = plan->shape(frame_of(k));
+      layouts[k] = parse_chunk(algorithm, static_cast<const uint8_t *>(chunks[k]), nbytes[k],
+                               static_cast<size_t>(sh.height) * sh.width, eb);
+    };
+    if (n > 1) {
+      if (!pool) {
+        const unsigned hw = std::thread::hardware_concurrency();
+        pool = std::make_unique<HostPool>(static_cast<int>(std::min(7u, hw > 1 ? hw - 1 : 1u)));
+      }
+      pool->run(n, parse);
+    } else if (n == 1) {
+      parse(0);
+    }
+    check(cudaStreamWaitEvent(copy, consumed[slot], 0), "ordering after the last run");
+    for (size_t k = 0; k < n; k++) {
+      const ThresholdPlan::Shape &sh = plan->shape(frame_of(k));
+      decoder.enqueue(static_cast<const uint8_t *>(chunks[k]), nbytes[k], layouts[k], sh.height,
+                      sh.width, plan->frame_origin(slot, frame_of(k)), plan->pitch() * eb, copy);
+    }
+    check(cudaEventRecord(uploaded[slot], copy), "cudaEventRecord");
   }
 
   void upload_chunk(int slot, int frame, const void *chunk, size_t nbytes, int algorithm) {

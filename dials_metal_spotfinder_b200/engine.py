@@ -78,6 +78,25 @@ class Engine:
         raise_for(lib.sf_engine_upload_chunk(self._h, slot, frame, chunk.ctypes.data, len(chunk),
                                              algorithm_code(algorithm)), "upload_chunk")
 
+    def upload_chunks(self, slot: int, chunks, frames=None, algorithm="bslz4") -> None:
+        """Several compressed frames at once (chunk k to frame frames[k], or
+        to frame k): their framing is checked on host threads in parallel,
+        all before any is enqueued. Keep the chunks alive until the next
+        synchronize()."""
+        from .chunk import algorithm_code
+        chunks = [np.ascontiguousarray(c, dtype=np.uint8) for c in chunks]
+        n = len(chunks)
+        ptrs = (ctypes.c_void_p * max(n, 1))(*[c.ctypes.data for c in chunks])
+        sizes = (ctypes.c_size_t * max(n, 1))(*[len(c) for c in chunks])
+        fr = None
+        if frames is not None:
+            if len(frames) != n:
+                raise ValueError("one frame number per chunk")
+            fr = (ctypes.c_int * max(n, 1))(*[int(f) for f in frames])
+        self._keep = chunks  # alive until the copies are done
+        raise_for(lib.sf_engine_upload_chunks(self._h, slot, n, fr, ptrs, sizes,
+                                              algorithm_code(algorithm)), "upload_chunks")
+
     def set_pixel_mask(self, frame: int, mask) -> None:
         """Frame `frame`'s pixel mask (nonzero = masked), stamped as the masked
         sentinel before every threshold; None clears it."""

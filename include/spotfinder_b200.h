@@ -260,6 +260,14 @@ SF_API int sf_engine_upload_device(sf_engine *engine, int slot, int frame,
  * unchanged until the next synchronize. */
 SF_API int sf_engine_upload_chunk(sf_engine *engine, int slot, int frame, const void *chunk,
                                   size_t nbytes, int algorithm);
+/* `count` chunks at once, chunk k for frame frames[k] (frame k with a null
+ * `frames`): the same as count sf_engine_upload_chunk calls, but the
+ * framing of every chunk is checked on host threads in parallel first, and
+ * a mismatch in any (-1) enqueues none. Extends the reference's per-frame
+ * decompress::image (src/decompress.hh:14-31) to a batch. */
+SF_API int sf_engine_upload_chunks(sf_engine *engine, int slot, size_t count, const int *frames,
+                                   const void *const *chunks, const size_t *nbytes,
+                                   int algorithm);
 /* The detector's pixel mask for frame `frame` (height x width bytes,
  * nonzero = a pixel not to use, as NXmx /entry/instrument/detector/
  * pixel_mask marks them), stamped into the frame as the masked sentinel

@@ -37,6 +37,9 @@ def fake_engine(sf):
         def upload(self, slot, frame, image):
             assert image.shape == self.shapes[frame]
 
+        def upload_chunks(self, slot, chunks, frames=None, algorithm="bslz4"):
+            assert len(chunks) == len(self.shapes)
+
         def synchronize(self):
             pass
 
@@ -127,3 +130,5 @@ def test_bench_line_has_the_contract_keys(monkeypatch):
     assert e["d2h_bytes_per_step"] == 7 * sf.SPOT.itemsize + 40 * sf.PIXEL.itemsize
     assert d["gpu_launches"] > 0 and d["gpu_launches"] % d["steps"] == 0
     assert d["gpixels_per_s"] > 0 and d["pipeline_bytes"]["per_frame"] > 0
+    c = d["e2e_chunks"]
+    assert c["value"] > 0 and 0 < c["h2d_bytes_per_step"] < e["h2d_bytes_per_step"]

@@ -333,3 +333,50 @@ def test_device_decode_large_lz4_blocks(gpu_lib, block):
     C.decode_device(ch, img.shape, np.uint16, dev.data_ptr(), pitch, "lz4")
     got = dev.cpu().numpy().reshape(517, pitch)[:, :1031 * 2].copy().view(np.uint16)
     assert np.array_equal(got, img)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("algorithm", ["lz4", "bslz4"])
+def test_batched_chunk_uploads_match_the_oracle(gpu_lib, algorithm):
+    """upload_chunks: every frame of the batch, in any frame order, gives the
+    oracle's list, as per-frame upload_chunk does; twice, so the staging
+    and table rings wrap."""
+    from dials_metal_spotfinder_b200.engine import Engine
+    from oracle import oracle as O
+    rng = np.random.default_rng(21)
+    shape = (517, 733)
+    imgs = []
+    for _ in range(6):
+        img = rng.poisson(1.4, shape).astype(np.uint16)
+        img[rng.random(shape) < 0.004] = rng.integers(200, 30000)
+        imgs.append(img)
+    chunks = [C.encode(img, algorithm) for img in imgs]
+    order = [3, 0, 5, 1, 4, 2]
+    with Engine([shape] * 6, np.uint16, slots=2) as eng:
+        for rep in range(3):
+            eng.upload_chunks(rep % 2, [chunks[f] for f in order], frames=order,
+                              algorithm=algorithm)
+            eng.run(rep % 2)
+            eng.synchronize()
+            for f, img in enumerate(imgs):
+                assert eng.signal(rep % 2, f).tobytes() == O.dext(img)[1].tobytes()
+
+
+@pytest.mark.gpu
+def test_batched_chunk_uploads_refuse_every_chunk_for_one_bad_one(gpu_lib):
+    from dials_metal_spotfinder_b200.engine import Engine
+    from oracle import oracle as O
+    rng = np.random.default_rng(22)
+    shape = (256, 384)
+    imgs = [rng.poisson(2.0, shape).astype(np.uint16) for _ in range(3)]
+    good = [C.encode(img, "bslz4") for img in imgs]
+    bad = good[:]
+    bad[1] = good[1][:-3]  # framing no longer describes the frame
+    with Engine([shape] * 3, np.uint16) as eng:
+        with pytest.raises(BadArgument):
+            eng.upload_chunks(0, bad)
+        eng.upload_chunks(0, good)
+        eng.run(0)
+        eng.synchronize()
+        for f, img in enumerate(imgs):
+            assert eng.signal(0, f).tobytes() == O.dext(img)[1].tobytes()
