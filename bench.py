@@ -176,10 +176,27 @@ class ClockSampler:
 
 # -- data -------------------------------------------------------------------
 
-def make_pool(n: int):
-    from dials_metal_spotfinder_b200 import synth
-    series = synth.eiger_16m(frames=max(n, 3))
-    return [series.frame(f) for f in range(n)]
+def load_synth():
+    """The synthetic-series module on its own, without importing the package
+    (whose import maps the product library): the reference arm must run with
+    nothing of the product loaded."""
+    import importlib.util
+    name = "_spotfinder_synth"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(
+        name, os.path.join(ROOT, "dials_metal_spotfinder_b200", "synth.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def make_pool(n: int, dtype=np.uint16):
+    from concurrent.futures import ThreadPoolExecutor
+    series = load_synth().eiger_16m(frames=max(n, 3), dtype=dtype)
+    with ThreadPoolExecutor(min(16, os.cpu_count() or 1)) as ex:
+        return list(ex.map(series.frame, range(n)))
 
 
 def measured_peaks():
@@ -224,11 +241,26 @@ def cpu_reference(frames, threads):
 
 # -- arms -------------------------------------------------------------------
 
+def mapped_libraries():
+    """The shared objects of this repository mapped into the process."""
+    found = set()
+    try:
+        with open("/proc/self/maps") as fh:
+            for line in fh:
+                path = line.split()[-1] if len(line.split()) >= 6 else ""
+                if path.endswith(".so") and os.path.realpath(path).startswith(
+                        os.path.realpath(ROOT)):
+                    found.add(os.path.relpath(os.path.realpath(path), os.path.realpath(ROOT)))
+    except OSError:
+        pass
+    return sorted(found)
+
+
 def run_reference_arm(args, ranks):
     if ranks.rank != 0:
         return
     threads = os.cpu_count() or 1
-    n = max(2, args.cpu_frames)
+    n = args.batch  # the same frames per step as the product arm
     frames = make_pool(n)
     for _ in range(max(0, min(args.warmup, 1))):
         cpu_reference(frames[:2], threads)
@@ -240,6 +272,7 @@ def run_reference_arm(args, ranks):
             break
     value = n * len(times) / sum(times)
     print(json.dumps({
+        "mapped_libraries": mapped_libraries(),
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
         "n_gpus": args.gpus, "steps": len(times), "warmup": args.warmup,
         "ms_per_step": 1000 * sum(times) / len(times), "higher_is_better": True,
@@ -514,8 +547,58 @@ def run_ours(args, ranks):
         "cpu_baseline": cpu,
     }
     eng.close()
+    # the step's output checked against the oracle, outside every timed region
+    line["parity"] = parity_check(pool, F) if ranks.rank == 0 else None
     if ranks.rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def parity_check(pool, F):
+    """Two steps of the timed form -- the same engine configuration (F frames
+    per run, two slots, 3D grouping with components carried between runs) on
+    the bench's first 2F frames, then finish -- against the oracle's dext +
+    Labeller on the same frames: every signal list of the second step, every
+    spot field and pixel, and the counts. Returns "ok" or what differed."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from dials_metal_spotfinder_b200.engine import Engine
+    from oracle import oracle as O
+    frames = [pool[i % len(pool)] for i in range(2 * F)]
+    spots, pixels = [], []
+    with Engine([SHAPE] * F, np.uint16, slots=2) as eng:
+        eng.enable_grouping(first_frame=0)
+        for b in range(2):
+            for f in range(F):
+                eng.upload(b, f, frames[b * F + f])
+            eng.run(b)
+            spots.append(eng.spots())
+            pixels.append(eng.pixels())
+        lists = [eng.signal(1, f) for f in range(F)]
+        eng.finish()
+        spots.append(eng.spots())
+        pixels.append(eng.pixels())
+        counts, _ = eng.group_counts()
+    spots, pixels = np.concatenate(spots), np.concatenate(pixels)
+    with ThreadPoolExecutor(os.cpu_count() or 1) as ex:
+        want_lists = [sig for _, sig, _ in ex.map(O.dext, frames)]
+    want = O.group(want_lists, *SHAPE)
+    out = {"frames": 2 * F, "spots": len(spots), "pixels": len(pixels),
+           "against": "oracle dext + Labeller (C restatement of src/dext.cc, "
+                      "src/dials_spots.cc)"}
+    bad = [f for f in range(F) if lists[f].tobytes() != want_lists[F + f].tobytes()]
+    if bad:
+        out["status"] = f"signal lists differ on frames {bad}"
+    elif counts != want.counts:
+        out["status"] = f"counts differ: {counts} vs {want.counts}"
+    elif len(spots) != len(want.spots) or any(
+            np.ascontiguousarray(spots[k]).tobytes() !=
+            np.ascontiguousarray(want.spots[k]).tobytes() for k in want.spots.dtype.names):
+        out["status"] = "spot fields differ"
+    elif pixels.tobytes() != want.pixels.tobytes():
+        out["status"] = "pixels differ"
+    else:
+        out["status"] = "ok"
+    return out
 
 
 def batched_vs_plain_4m(steps: int = 10):

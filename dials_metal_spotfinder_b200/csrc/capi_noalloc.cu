@@ -25,7 +25,8 @@
 // Every call shares the array, and the array keeps what the last call left
 // in it, so each call clears what must start at zero (the tile counts, the
 // pool cursor, the status and count words) and refills the arena's masked
-// margins. Calls whose device work overlapped would race on the array; each
+// margins, unless the previous completed call on that device had the same
+// frame shape and so left them intact. Calls whose device work overlapped would race on the array; each
 // call therefore holds a process-wide lock and returns only when its stream
 // is idle, so calls through this entry point never overlap. Nothing here
 // calls cudaMalloc, cudaFree, cudaMallocHost or any allocating library
@@ -53,6 +54,10 @@ constexpr int kBlocksPerSm = 2; // bounds the staging pool: one open chunk per w
 
 std::mutex g_lock;
 void *g_scratch_ptr[kMaxDevices] = {};
+// The frame shape whose arena margins the scratch holds on each device
+// (0 x 0: none, or not known to be intact), so that a run of calls with one
+// shape fills the margins once.
+size_t g_filled_h[kMaxDevices] = {}, g_filled_w[kMaxDevices] = {};
 
 uint64_t align_up(uint64_t v, uint64_t m) { return (v + m - 1) / m * m; }
 
@@ -163,6 +168,8 @@ int find_noalloc(const uint16_t *image, size_t height, size_t width, SignalPixel
     return -1;
   const std::lock_guard<std::mutex> hold(g_lock);
   unsigned char *base = scratch_address();
+  int dev = 0;
+  check(cudaGetDevice(&dev), "cudaGetDevice");
   const Layout L = plan_layout(height, width);
   if (L.total > kScratchBytes) {
     set_error(("a " + std::to_string(height) + " x " + std::to_string(width) +
@@ -195,11 +202,20 @@ int find_noalloc(const uint16_t *image, size_t height, size_t width, SignalPixel
   check(cudaMemsetAsync(pool_next, 0, 16, s), "clearing the pool cursor");
   check(cudaMemsetAsync(count, 0, 2 * 4, s), "clearing the count and status");
   // Off-frame pixels read as masked: every byte of the arena that the frame
-  // does not cover is 0xFF.
-  check(cudaMemsetAsync(arena, 0xff, L.arena_bytes, s), "filling the arena");
+  // does not cover is 0xFF. The layout is a function of the shape and only
+  // the frame's own pixels are written below, so after a completed call with
+  // the same shape the margins are still 0xFF and the fill is skipped. The
+  // record is cleared first and set again only once this call completes, so
+  // a call that fails part-way makes the next one fill.
+  const bool filled = g_filled_h[dev] == height && g_filled_w[dev] == width;
+  g_filled_h[dev] = g_filled_w[dev] = 0;
+  if (!filled)
+    check(cudaMemsetAsync(arena, 0xff, L.arena_bytes, s), "filling the arena");
   const uint64_t origin = (static_cast<uint64_t>(L.frame.row0) * L.pitch + kMarginLeft) * 2;
+  // cudaMemcpyDefault, as sf_find_u16 uses: the image may be host, device or
+  // managed memory.
   check(cudaMemcpy2DAsync(static_cast<unsigned char *>(arena) + origin, L.pitch * 2, image,
-                          width * 2, width * 2, height, cudaMemcpyHostToDevice, s),
+                          width * 2, width * 2, height, cudaMemcpyDefault, s),
         "copying the frame to the device");
 
   CUtensorMap map;
@@ -238,13 +254,14 @@ int find_noalloc(const uint16_t *image, size_t height, size_t width, SignalPixel
   check(cudaStreamSynchronize(s), "cudaStreamSynchronize");
   if (static_cast<int>(host_words[1]) == kStatusTmaTimeout)
     throw DeviceError("a TMA load did not complete in time");
+  g_filled_h[dev] = height;
+  g_filled_w[dev] = width;
   *found = host_words[0];
   if (host_words[0] > L.frame.capacity || host_words[0] > capacity)
     return -2;
   if (host_words[0] == 0)
     return 0;
-  check(cudaMemcpyAsync(out, list, host_words[0] * sizeof(SignalPixel), cudaMemcpyDeviceToHost,
-                        s),
+  check(cudaMemcpyAsync(out, list, host_words[0] * sizeof(SignalPixel), cudaMemcpyDefault, s),
         "copying the signal pixels back");
   check(cudaStreamSynchronize(s), "cudaStreamSynchronize");
   return 0;

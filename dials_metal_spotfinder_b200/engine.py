@@ -31,6 +31,7 @@ class Engine:
         raise_for(status, "sf_engine_create")
         self._h = handle
         self.slots = slots
+        self._keep = {}
 
     def close(self):
         if getattr(self, "_h", None):
@@ -93,7 +94,9 @@ class Engine:
             if len(frames) != n:
                 raise ValueError("one frame number per chunk")
             fr = (ctypes.c_int * max(n, 1))(*[int(f) for f in frames])
-        self._keep = chunks  # alive until the copies are done
+        # Alive until the copies are done: one list per slot, dropped by
+        # synchronize(), so a slot still in flight keeps its chunks.
+        self._keep[slot] = chunks
         raise_for(lib.sf_engine_upload_chunks(self._h, slot, n, fr, ptrs, sizes,
                                               algorithm_code(algorithm)), "upload_chunks")
 
@@ -116,6 +119,7 @@ class Engine:
 
     def synchronize(self) -> None:
         raise_for(lib.sf_engine_synchronize(self._h), "synchronize")
+        self._keep.clear()
 
     def counts(self, slot: int = 0) -> np.ndarray:
         out = np.zeros(self.nframes, np.uint32)

@@ -13,7 +13,7 @@
  * The reference interface each entry point replaces is cited beside it
  * (paths are within graeme-winter/dials-metal-spotfinder). The C++ drop-in
  * for the reference's own gpu:: interface (include/dext_gpu.hh) is built on
- * these functions; INTEGRATION.md shows the bindings.
+ * these functions.
  *
  * Threading: sf_find_* may be called concurrently from many host threads; each
  * thread gets its own stream and device buffers, as the reference's per-thread

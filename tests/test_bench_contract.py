@@ -99,6 +99,7 @@ def test_bench_line_has_the_contract_keys(monkeypatch):
     monkeypatch.setattr(sf, "find", lambda image, out=None: np.zeros(0, sf.SIGNAL_PIXEL))
     monkeypatch.setattr(_lib, "raise_for", lambda status, what: None)
     monkeypatch.setattr(bench, "reference_gpu_form", lambda frame: {"unavailable": "fake"})
+    monkeypatch.setattr(bench, "parity_check", lambda pool, F: {"status": "fake"})
     monkeypatch.setattr(bench, "make_pool",
                         lambda n: [np.zeros(bench.SHAPE, np.uint16) for _ in range(n)])
     monkeypatch.setattr(sys, "argv", ["bench.py", "--steps", "2", "--warmup", "3", "--no-cpu",
@@ -112,7 +113,7 @@ def test_bench_line_has_the_contract_keys(monkeypatch):
     d = json.loads(lines[0])
     for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
                 "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "config",
-                "roofline", "clocks", "gpu_launches", "e2e", "cpu_baseline"):
+                "roofline", "clocks", "gpu_launches", "e2e", "cpu_baseline", "parity"):
         assert key in d, key
     assert d["n_gpus"] == 1 and d["steps"] == 2 and d["warmup"] == 3
     assert d["higher_is_better"] is True and d["scaling"] == "weak"

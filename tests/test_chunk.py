@@ -7,7 +7,8 @@ which is vendored (its third_party/bitshuffle submodule is empty). The LZ4
 blocks are pinned against the system's liblz4 (LZ4_compress_default /
 LZ4_decompress_safe, called through its public API) where it is installed;
 the bit transpose against a numpy restatement of the published layout (bit
-k of byte j of element e at bit e mod 8 of byte e / 8 of row 8j + k).
+k of byte j of element e at bit e mod 8 of byte e / 8 of row 8j + k) and
+against a chunk worked out by hand from the published formats.
 Host tests need no device; the device decoder's tests are marked gpu."""
 
 import ctypes
@@ -76,6 +77,89 @@ def bit_transpose(block: np.ndarray) -> bytes:
     bits = np.unpackbits(b, axis=1, bitorder="little")       # [element][8*byte + bit]
     rows = bits.T.reshape(8 * s, n // 8, 8)                 # [row][group][element % 8]
     return np.packbits(rows, axis=2, bitorder="little").reshape(-1).tobytes()
+
+
+def liblz4_chunk(img: np.ndarray, algorithm: str, block_bytes: int) -> np.ndarray:
+    """A chunk in the HDF5 filter framing with any block size, its blocks
+    compressed by liblz4 and, for bslz4, bit-transposed by the numpy
+    restatement above (the trailing elements past a multiple of 8 copied
+    as they are)."""
+    s = img.dtype.itemsize
+    flat = img.reshape(-1)
+    raw = flat.view(np.uint8).tobytes()
+    out = bytearray(struct.pack(">QI", len(raw), block_bytes))
+
+    def emit(src: bytes):
+        dst = ctypes.create_string_buffer(len(src) + len(src) // 255 + 64)
+        cs = LZ4.LZ4_compress_default(src, dst, len(src), len(dst))
+        assert cs > 0
+        out.extend(struct.pack(">I", cs) + dst.raw[:cs])
+
+    if algorithm == "lz4":
+        for at in range(0, len(raw), block_bytes):
+            emit(raw[at:at + block_bytes])
+    else:
+        per = block_bytes // s
+        coded = len(flat) - len(flat) % 8
+        for at in range(0, coded, per):
+            emit(bit_transpose(flat[at:min(at + per, coded)]))
+        out.extend(flat[coded:].view(np.uint8).tobytes())
+    return np.frombuffer(bytes(out), np.uint8)
+
+
+# A bitshuffle + LZ4 chunk worked out by hand from the published formats,
+# not by any encoder here. The frame is 1 x 8 uint16 pixels
+#     0x0001 0x0003 0x0000 0x8000 0x00ff 0x0100 0x0000 0xffff
+# Low bytes by element:  01 03 00 00 ff 00 00 ff; high bytes: 00 00 00 80 00 01 00 ff.
+# Bitshuffle writes, for byte j and bit k of the element, row 8j + k: one bit
+# per element, element e at bit e mod 8 of byte e / 8 (8 elements: one byte
+# per row, 16 rows).
+#   row 0 (bit 0 of the low bytes): elements 0, 1, 4, 7    -> 0b10010011 = 0x93
+#   row 1 (bit 1):                  elements 1, 4, 7       -> 0x92
+#   rows 2-7:                       elements 4, 7          -> 0x90 each
+#   row 8 (bit 0 of the high bytes): elements 5, 7         -> 0xa0
+#   rows 9-14:                      element 7              -> 0x80 each
+#   row 15 (bit 7):                 elements 3, 7          -> 0x88
+# The LZ4 block holds those 16 bytes as one literals-only sequence: token
+# 0xf0 (15 literals and more, no match), length byte 0x01 (15 + 1 = 16),
+# then the 16 bytes. The HDF5 bitshuffle filter's framing before it: the
+# uncompressed size as 8 big-endian bytes (16), the block size as 4 (8192
+# bytes), then the block's compressed length as 4 (18).
+HAND_FRAME = np.array([[0x0001, 0x0003, 0x0000, 0x8000, 0x00ff, 0x0100, 0x0000, 0xffff]],
+                      np.uint16)
+HAND_ROWS = bytes([0x93, 0x92] + [0x90] * 6 + [0xa0] + [0x80] * 6 + [0x88])
+HAND_CHUNK = bytes.fromhex("0000000000000010" "00002000" "00000012" "f001") + HAND_ROWS
+
+
+def test_hand_derived_bitshuffle_chunk_decodes():
+    assert bit_transpose(HAND_FRAME.reshape(-1)) == HAND_ROWS
+    got = C.decode(np.frombuffer(HAND_CHUNK, np.uint8), HAND_FRAME.shape, np.uint16, "bslz4")
+    assert np.array_equal(got, HAND_FRAME)
+    # the same eight pixels with two more after them: those two are not
+    # transposed (not a whole group of 8) and follow the blocks as they are
+    frame10 = np.concatenate([HAND_FRAME, [[0x1234, 0xabcd]]], axis=1).astype(np.uint16)
+    chunk10 = (bytes.fromhex("0000000000000014" "00002000" "00000012" "f001") + HAND_ROWS +
+               bytes.fromhex("3412" "cdab"))
+    got = C.decode(np.frombuffer(chunk10, np.uint8), frame10.shape, np.uint16, "bslz4")
+    assert np.array_equal(got, frame10)
+
+
+@needs_liblz4
+def test_our_bslz4_chunk_of_the_hand_frame_is_the_hand_rows():
+    chunk = bytes(C.encode(HAND_FRAME, "bslz4"))
+    size, block, parts, rest = split_blocks(chunk, 16)
+    assert (size, len(parts), rest) == (16, 1, b"")
+    dst = ctypes.create_string_buffer(16)
+    assert LZ4.LZ4_decompress_safe(parts[0], dst, len(parts[0]), 16) == 16
+    assert dst.raw == HAND_ROWS
+
+
+@needs_liblz4
+@pytest.mark.parametrize("algorithm", ["lz4", "bslz4"])
+def test_liblz4_chunks_with_small_blocks_decode_with_ours(algorithm):
+    for img in frames():
+        chunk = liblz4_chunk(img, algorithm, 256 * img.dtype.itemsize)
+        assert np.array_equal(C.decode(chunk, img.shape, img.dtype, algorithm), img)
 
 
 @pytest.mark.parametrize("algorithm", ["raw", "lz4", "bslz4"])
@@ -213,6 +297,15 @@ def test_device_decode_feeds_the_engine(gpu_lib, algorithm):
 
 
 @pytest.mark.gpu
+def test_device_decodes_the_hand_derived_chunk(gpu_lib):
+    import torch
+    dev = torch.zeros(HAND_FRAME.shape, dtype=torch.uint16, device="cuda")
+    C.decode_device(np.frombuffer(HAND_CHUNK, np.uint8), HAND_FRAME.shape, np.uint16,
+                    dev.data_ptr())
+    assert np.array_equal(dev.cpu().numpy(), HAND_FRAME)
+
+
+@pytest.mark.gpu
 def test_device_decode_u32(gpu_lib):
     from dials_metal_spotfinder_b200.engine import Engine
     from oracle import oracle as O
@@ -336,11 +429,14 @@ def test_device_decode_large_lz4_blocks(gpu_lib, block):
 
 
 @pytest.mark.gpu
+@needs_liblz4
 @pytest.mark.parametrize("algorithm", ["lz4", "bslz4"])
 def test_batched_chunk_uploads_match_the_oracle(gpu_lib, algorithm):
     """upload_chunks: every frame of the batch, in any frame order, gives the
-    oracle's list, as per-frame upload_chunk does; twice, so the staging
-    and table rings wrap."""
+    oracle's list, as per-frame upload_chunk does. Eight batches of six
+    chunks (48 uploads) wrap the 32-deep block-table ring; the last three
+    batches use frames with smaller LZ4 blocks, so more blocks per chunk,
+    and a table still in use must grow."""
     from dials_metal_spotfinder_b200.engine import Engine
     from oracle import oracle as O
     rng = np.random.default_rng(21)
@@ -351,10 +447,13 @@ def test_batched_chunk_uploads_match_the_oracle(gpu_lib, algorithm):
         img[rng.random(shape) < 0.004] = rng.integers(200, 30000)
         imgs.append(img)
     chunks = [C.encode(img, algorithm) for img in imgs]
+    # 1 KB blocks: eight times as many per chunk as the encoder's 8 KB
+    small = [liblz4_chunk(img, algorithm, 1024) for img in imgs]
     order = [3, 0, 5, 1, 4, 2]
     with Engine([shape] * 6, np.uint16, slots=2) as eng:
-        for rep in range(3):
-            eng.upload_chunks(rep % 2, [chunks[f] for f in order], frames=order,
+        for rep in range(8):
+            use = small if rep >= 5 else chunks
+            eng.upload_chunks(rep % 2, [use[f] for f in order], frames=order,
                               algorithm=algorithm)
             eng.run(rep % 2)
             eng.synchronize()

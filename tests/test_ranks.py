@@ -57,7 +57,7 @@ def test_reference_arm_under_two_ranks():
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(port), "bench.py",
            "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "0",
-           "--cpu-frames", "2"]
+           "--batch", "2"]
     p = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert p.returncode == 0, p.stderr[-2000:]
     lines = [l for l in p.stdout.splitlines() if l.startswith("{")]
@@ -65,3 +65,6 @@ def test_reference_arm_under_two_ranks():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["cpu_baseline"]["cores"] >= 1
+    # the arm runs the reference's code alone: nothing of the product mapped
+    assert d["config"]["frames_per_step"] == 2
+    assert not any("spotfinder_b200" in lib for lib in d["mapped_libraries"])

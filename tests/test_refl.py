@@ -20,7 +20,11 @@ from refl_reader import read, shoeboxes
 CASES = [("refl_small.refl", "3d", "golden", 0, True),
          ("refl_small_2d.refl", "2d", "", 0, True),
          ("refl_small_noshoebox.refl", "3d", "golden-3", 3, False)]
-CHECK_REFL = "/root/reference/tests/check_refl.py"
+# The reference tree: $SPOTFINDER_REFERENCE, else a `reference` directory
+# beside this repository. Absent on a machine without it (the test skips).
+REFERENCE = os.environ.get("SPOTFINDER_REFERENCE") or os.path.join(
+    os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))), "reference")
+CHECK_REFL = os.path.join(REFERENCE, "tests", "check_refl.py")
 COLUMNS = {"bbox": "int6", "flags": "std::size_t", "id": "int", "intensity.sum.value": "double",
            "intensity.sum.variance": "double", "n_signal": "int", "panel": "std::size_t",
            "shoebox": "Shoebox<>", "xyzobs.px.value": "vec3<double>",
