@@ -52,7 +52,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--batch", type=int, default=0,
+                    help="frames per launch; 0: the autotuner's choice (8 to 32)")
     # Distinct consecutive frames of one series, cycled. With grouping in the
     # step the cycle must be longer than any reflection's extent in z (about
     # ten frames here): a reflection present at both ends of a short cycle
@@ -61,11 +62,14 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=8)
     ap.add_argument("--cpu-frames", type=int, default=8)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--serve-seconds", type=float, default=3.0,
+    ap.add_argument("--serve-seconds", type=float, default=60.0,
                     help="length of the two-stream serving replay (0: skip)")
-    ap.add_argument("--plain-seconds", type=float, default=0.5,
+    ap.add_argument("--plain-seconds", type=float, default=10.0,
                     help="length of the plain per-frame replay of the same streams")
     ap.add_argument("--no-4m", action="store_true")
+    ap.add_argument("--no-u32", action="store_true")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="skip the autotuner (frames per launch 16 unless --batch)")
     return ap.parse_args()
 
 
@@ -260,7 +264,9 @@ def run_reference_arm(args, ranks):
     if ranks.rank != 0:
         return
     threads = os.cpu_count() or 1
-    n = args.batch  # the same frames per step as the product arm
+    # the same frames per step as the product arm (whose autotuner picks 16
+    # on these frames; --batch fixes both arms)
+    n = args.batch or 16
     frames = make_pool(n)
     for _ in range(max(0, min(args.warmup, 1))):
         cpu_reference(frames[:2], threads)
@@ -292,12 +298,21 @@ def run_ours(args, ranks):
     from dials_metal_spotfinder_b200.engine import Engine
 
     _lib.raise_for(_lib.lib.sf_set_device(ranks.local), "sf_set_device")
-    F = args.batch
     pool = make_pool(args.pool)
     frame_bytes = SHAPE[0] * SHAPE[1] * 2
+    # frames per launch, warps per block and task height from the autotuner
+    # (a timed search, or its tuner file when this device has one)
+    tuning = None
+    if not args.no_tune:
+        from dials_metal_spotfinder_b200.tune import tune
+        t0 = time.perf_counter()
+        tuning = tune(pool[:16], min_frames=8, max_frames=32)
+        tuning["seconds"] = time.perf_counter() - t0
+    F = args.batch or (tuning["frames_per_launch"] if tuning else 16)
     eng = Engine([SHAPE] * F, np.uint16, slots=2)
     eng.enable_grouping(first_frame=0)
     info = eng.info()
+    engine_tuning = eng.tuning()
     for s in range(2):
         for f in range(F):
             eng.upload(s, f, pool[(s * F + f) % len(pool)])
@@ -474,6 +489,10 @@ def run_ours(args, ranks):
     if ranks.rank == 0 and not args.no_4m:
         four_m = batched_vs_plain_4m()
 
+    u32 = None
+    if ranks.rank == 0 and not args.no_u32:
+        u32 = u32_16m(args.steps)
+
     served = None
     if ranks.rank == 0 and args.serve_seconds > 0:
         served = serving(args.serve_seconds, args.plain_seconds, pool)
@@ -509,6 +528,7 @@ def run_ours(args, ranks):
                    "l2": "inputs larger than L2 (580 MB per step)",
                    "parallelism": f"replicas x{ranks.world}",
                    "engine": info},
+        "tuning": {"search": tuning, "engine": engine_tuning},
         "graph_replay": {"value": frames_total / (graph_ms / 1000.0), "unit": UNIT,
                          "ms_per_step": graph_ms / args.steps},
         "grouping": {"spots_per_frame": spots_per_frame,
@@ -536,6 +556,7 @@ def run_ours(args, ranks):
         "plain_gpu": plain,
         "reference_gpu": ref_gpu,
         "batched_vs_plain_4m": four_m,
+        "u32_16m": u32,
         "latency": ({"frame_to_mask_p99_ms": {
                         name: r["frame_to_mask_ms"]["p99"]
                         for name, r in zip(("4m_500hz", "16m_100hz"), served["served"])},
@@ -601,26 +622,116 @@ def parity_check(pool, F):
     return out
 
 
-def batched_vs_plain_4m(steps: int = 10):
-    """4M-shaped frames (2162 x 2068): the batched engine (16 frames per
-    launch, resident, with 3D grouping, graph replay) against the plain
-    per-frame form (sf_find_u16 per frame from pinned host memory) on the
-    same frames, frames/s each."""
+def batched_vs_plain_4m(steps: int = 12):
+    """4M-shaped frames (2162 x 2068), the batched engine (16 frames per
+    launch) against the plain per-frame form (sf_find_u16, one frame per
+    call), like for like: both fed from the same page-locked host frames,
+    both returning their results to page-locked host memory, both timed on
+    the host wall clock over the same work.
+
+    threshold: the signal lists only -- batched: upload 16 frames, run
+    without grouping, read the 16 lists (one call), step i+1's upload
+    overlapping step i's run and read; plain: sf_find_u16 per frame.
+    grouped: threshold + 3D grouping, the finished spots and their pixels
+    returned -- batched: the engine with grouping; plain: sf_find_u16 per
+    frame then the device labeller's add (sf_labeller_add), the reference
+    CLI's per-frame order (src/find_spots.cc:243-264,550-591)."""
     import dials_metal_spotfinder_b200 as sf
-    from dials_metal_spotfinder_b200 import synth
     from dials_metal_spotfinder_b200.engine import Engine
-    series = synth.eiger_4m(frames=32)
+    from dials_metal_spotfinder_b200.labeller import Labeller
+    series = load_synth().eiger_4m(frames=32)
     pool = [series.frame(f) for f in range(32)]
     shape = pool[0].shape
     F = 16
-    with Engine([shape] * F, np.uint16, slots=2) as eng:
+    cap = shape[0] * shape[1] * 2 // 16
+    hb = [sf.HostBuffer(shape, np.uint16) for _ in range(32)]
+    for f in range(32):
+        hb[f].array[:] = pool[f]
+    lists = sf.HostBuffer((F * cap,), sf.SIGNAL_PIXEL)
+    one = sf.HostBuffer((cap,), sf.SIGNAL_PIXEL)
+    spot_buf = sf.HostBuffer((1 << 18,), sf.SPOT)
+    pix_buf = sf.HostBuffer((1 << 22,), sf.PIXEL)
+    out = {"workload": "4M-shaped uint16 frames, 2162x2068", "unit": UNIT,
+           "timer": "host wall clock, synchronised at both ends",
+           "input": "page-locked host frames, 32 distinct, cycled",
+           "batched_form": "engine, 16 frames per launch, two slots, step i+1 uploading "
+                           "while step i runs and reads back",
+           "plain_form": "sf_find_u16 per frame (upload, threshold, list back), one call "
+                         "after another"}
+
+    def batched(grouping):
+        with Engine([shape] * F, np.uint16, slots=2) as eng:
+            if grouping:
+                eng.enable_grouping(first_frame=0)
+
+            def upload(i):
+                for f in range(F):
+                    eng.upload(i % 2, f, hb[(i * F + f) % 32].array)
+
+            def read(i):
+                if grouping:
+                    eng.spots(out=spot_buf.array)
+                    eng.pixels(out=pix_buf.array)
+                else:
+                    eng.signals(i % 2, out=lists.array)
+
+            for rep in range(2):  # the first pass warms up
+                eng.synchronize()
+                t0 = time.perf_counter()
+                upload(0)
+                eng.run(0)
+                for i in range(1, steps):
+                    upload(i)
+                    read(i - 1)
+                    eng.run(i % 2)
+                read(steps - 1)
+                eng.synchronize()
+                dt = time.perf_counter() - t0
+            return F * steps / dt
+
+    def plain(grouping):
+        n = F * steps
+        lab = Labeller(*shape) if grouping else None
+        for rep in range(2):
+            t0 = time.perf_counter()
+            for i in range(n):
+                sig = sf.find(hb[i % 32].array, out=one.array)
+                if grouping:
+                    lab.add(rep * n + i, sig)
+            if grouping:  # the spots and pixels found so far, to the host
+                lab.spots()
+                lab.pixels()
+            dt = time.perf_counter() - t0
+        if lab:
+            lab.close()
+        return n / dt
+
+    try:
+        for name, grouping in (("threshold", False), ("grouped", True)):
+            b, p = batched(grouping), plain(grouping)
+            out[name] = {"batched": b, "plain": p, "ratio": b / p}
+    finally:
+        for b in hb + [lists, one, spot_buf, pix_buf]:
+            b.close()
+    return out
+
+
+def u32_16m(steps: int):
+    """The 16M uint32 variant (intensities up to 2e6): threshold + 3D
+    grouping through the batched engine, frames resident, CUDA events as the
+    headline's; the uint32 threshold kernel's roofline beside it."""
+    from dials_metal_spotfinder_b200.engine import Engine
+    F = 16
+    pool = make_pool(24, np.uint32)
+    shape = pool[0].shape
+    frame_bytes = shape[0] * shape[1] * 4
+    with Engine([shape] * F, np.uint32, slots=2) as eng:
         eng.enable_grouping(first_frame=0)
         for s in range(2):
             for f in range(F):
-                eng.upload(s, f, pool[s * F + f])
+                eng.upload(s, f, pool[(s * F + f) % len(pool)])
         eng.synchronize()
-        eng.use_graph(True)
-        for i in range(4):
+        for i in range(3):
             eng.run(i % 2)
         eng.synchronize()
         eng.record(0)
@@ -628,25 +739,29 @@ def batched_vs_plain_4m(steps: int = 10):
             eng.run(i % 2)
         eng.record(1)
         eng.synchronize()
-        batched = F * steps / (eng.elapsed_ms(0, 1) / 1e3)
-    hb = sf.HostBuffer(shape, np.uint16)
-    hb.array[:] = pool[0]
-    sig = sf.HostBuffer((shape[0] * shape[1] * 2 // 16,), sf.SIGNAL_PIXEL)
-    for _ in range(3):
-        sf.find(hb.array, out=sig.array)
-    n = 30
-    t0 = time.perf_counter()
-    for i in range(n):
-        sf.find(hb.array, out=sig.array)
-    plain = n / (time.perf_counter() - t0)
-    hb.close()
-    sig.close()
-    return {"workload": "4M-shaped uint16 frames, 2162x2068", "unit": UNIT,
-            "batched": batched, "plain": plain, "ratio": batched / plain,
-            "batched_form": "engine, 16 frames per launch, resident, threshold + 3D grouping, "
-                            "graph replay, CUDA events",
-            "plain_form": "sf_find_u16 per frame, pinned frame and signal list, threshold only, "
-                          "host wall clock"}
+        ms = eng.elapsed_ms(0, 1)
+        eng.profile(True)
+        for i in range(steps):
+            eng.run(i % 2)
+        eng.synchronize()
+        stage = eng.stage_totals()
+        eng.profile(False)
+        nsig = [int(eng.counts(s).sum()) for s in range(2)]
+    alg = statistics.mean(F * frame_bytes + 16 * n for n in nsig)
+    thr_ms = stage["threshold_ms"] / max(stage["runs"], 1)
+    peak, peak_kind = measured_peaks()
+    achieved = alg / (thr_ms / 1e3) / 1e9
+    return {"workload": "Eiger2-16M-shaped uint32 frames, 4362x4148, intensities up to 2e6, "
+                        "batched engine, threshold + 3D grouping",
+            "value": F * steps / (ms / 1e3), "unit": UNIT, "frames_per_step": F,
+            "ms_per_step": ms / steps, "signal_pixels_per_frame": statistics.mean(nsig) / F,
+            "stage_ms_per_step": {"threshold": thr_ms,
+                                  "placement": stage["place_ms"] / max(stage["runs"], 1),
+                                  "grouping": stage["group_ms"] / max(stage["runs"], 1)},
+            "roofline": {"bound": "hbm", "kernel": "threshold_kernel<uint32_t>",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "kernel_ms_per_launch": thr_ms, "algorithmic_bytes_per_launch": alg}}
 
 
 def serving(seconds: float, plain_seconds: float, pool16):
@@ -655,11 +770,10 @@ def serving(seconds: float, plain_seconds: float, pool16):
     100 Hz. Then the plain per-frame form (host decode, sf_find_u16,
     labeller) on the same streams for plain_seconds."""
     from dials_metal_spotfinder_b200 import chunk as C
-    from dials_metal_spotfinder_b200 import synth
     from dials_metal_spotfinder_b200.serve import Stream, drive, drive_plain
     # distinct frames cycled, longer than any reflection's z extent
     n = min(24, len(pool16))
-    s4 = synth.eiger_4m(frames=n)
+    s4 = load_synth().eiger_4m(frames=n)
     c4 = [C.encode(s4.frame(f), "bslz4") for f in range(n)]
     c16 = [C.encode(f, "bslz4") for f in pool16[:n]]
     raw4 = s4.height * s4.width * 2

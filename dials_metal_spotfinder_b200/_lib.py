@@ -117,6 +117,7 @@ SIGNATURES = {
     "sf_engine_synchronize": (_I, [_P]),
     "sf_engine_counts": (_I, [_P, _I, _P]),
     "sf_engine_signal": (_I, [_P, _I, _I, _P, _S, ctypes.POINTER(_S)]),
+    "sf_engine_signals": (_I, [_P, _I, _P, _S, _P]),
     "sf_engine_record": (_I, [_P, _I]),
     "sf_engine_elapsed": (_I, [_P, _I, _I, ctypes.POINTER(ctypes.c_float)]),
     "sf_engine_profile": (_I, [_P, _I]),
@@ -132,6 +133,8 @@ SIGNATURES = {
     "sf_engine_spots": (_I, [_P, _P, _S, ctypes.POINTER(_S)]),
     "sf_engine_pixels": (_I, [_P, _P, _S, ctypes.POINTER(_S)]),
     "sf_engine_finish": (_I, [_P]),
+    "sf_tune": (_I, [_I, _I, _I, _P, _I, _P, _P]),
+    "sf_engine_tuning": (_I, [_P, _P]),
 }
 
 
@@ -143,6 +146,23 @@ class ReflOptions(ctypes.Structure):
 class ServerConfig(ctypes.Structure):
     _fields_ = [("hbm_budget", ctypes.c_uint64), ("slots", ctypes.c_int32),
                 ("use_graph", ctypes.c_int32)]
+
+
+class TuneOptions(ctypes.Structure):
+    _fields_ = [("min_frames", ctypes.c_int32), ("max_frames", ctypes.c_int32),
+                ("steps", ctypes.c_int32), ("grouping", ctypes.c_int32),
+                ("use_cache", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("hbm_budget", ctypes.c_uint64), ("cache_path", ctypes.c_char_p)]
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [("frames_per_launch", ctypes.c_int32), ("warps_per_block", ctypes.c_int32),
+                ("seg_rows", ctypes.c_int32), ("from_cache", ctypes.c_int32),
+                ("candidates", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("seg_ratio", ctypes.c_double), ("us_per_frame", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
 
 
 class EngineConfig(ctypes.Structure):

@@ -74,19 +74,47 @@ int sf_engine_create(int elem_bytes, int nframes, const int32_t *heights,
     }
     sf::PlanTuning t;
     int slots = 1;
+    bool automatic = true;
     if (config) {
       t.seg_rows = config->seg_rows;
       t.warps_per_block = config->warps_per_block > 0 ? config->warps_per_block : 4;
       t.blocks_per_sm = config->blocks_per_sm;
       slots = config->slots > 0 ? config->slots : 1;
+      automatic = config->seg_rows == 0 && config->warps_per_block == 0;
+    }
+    bool uniform = true;
+    for (const auto &sh : shapes)
+      uniform = uniform && sh.height == shapes[0].height && sh.width == shapes[0].width;
+    sf::TuneEntry tuned;
+    const bool from_cache = automatic && uniform &&
+                            sf::tune_lookup(elem_bytes, shapes[0].height, shapes[0].width,
+                                            nullptr, &tuned);
+    if (from_cache) {
+      t.warps_per_block = tuned.warps_per_block;
+      t.seg_rows = sf::tune_seg_rows(elem_bytes, shapes, tuned.warps_per_block, tuned.seg_ratio);
     }
     auto e = sf::make_engine(elem_bytes, shapes, t, slots);
+    e->tuned_from_cache = from_cache;
     *out = reinterpret_cast<sf_engine *>(e.release());
     return 0;
   });
 }
 
 void sf_engine_destroy(sf_engine *engine) { delete reinterpret_cast<Engine *>(engine); }
+
+int sf_engine_tuning(sf_engine *engine, sf_tune_result *out) {
+  return guarded([&] {
+    if (!engine || !out)
+      return -1;
+    const Engine *e = reinterpret_cast<Engine *>(engine);
+    *out = sf_tune_result{};
+    out->frames_per_launch = e->plan->nframes();
+    out->warps_per_block = e->plan->tuning().warps_per_block;
+    out->seg_rows = e->plan->tuning().seg_rows;
+    out->from_cache = e->tuned_from_cache ? 1 : 0;
+    return 0;
+  });
+}
 
 int sf_engine_info(sf_engine *engine, int64_t *out8) {
   return guarded([&] {
@@ -188,6 +216,43 @@ int sf_engine_counts(sf_engine *engine, int slot, uint32_t *counts) {
     sf::check(cudaStreamSynchronize(e->compute), "cudaStreamSynchronize");
     for (int f = 0; f < nf; f++)
       counts[f] = e->pinned[f];
+    return 0;
+  });
+}
+
+int sf_engine_signals(sf_engine *engine, int slot, sf_signal_pixel *out, size_t capacity,
+                      uint32_t *counts) {
+  return guarded([&] {
+    if (!engine || !counts)
+      return -1;
+    Engine *e = reinterpret_cast<Engine *>(engine);
+    e->check_slot(slot);
+    const int nf = e->plan->nframes();
+    sf::check(cudaMemcpyAsync(e->pinned, e->plan->frame_count(slot), nf * sizeof(uint32_t),
+                              cudaMemcpyDeviceToHost, e->compute),
+              "reading the counts");
+    sf::check(cudaStreamSynchronize(e->compute), "cudaStreamSynchronize");
+    uint64_t total = 0;
+    bool over = false;
+    for (int f = 0; f < nf; f++) {
+      counts[f] = e->pinned[f];
+      over = over || counts[f] > e->plan->capacity(f);
+      total += counts[f];
+    }
+    if (over || total > capacity)
+      return -2;
+    if (total > 0 && !out)
+      return -1;
+    uint64_t at = 0;
+    for (int f = 0; f < nf; f++) {
+      if (counts[f])
+        sf::check(cudaMemcpyAsync(out + at, e->plan->out(slot) + e->plan->out_base(f),
+                                  counts[f] * sizeof(sf::SignalPixel), cudaMemcpyDeviceToHost,
+                                  e->compute),
+                  "copying the signal pixels back");
+      at += counts[f];
+    }
+    sf::check(cudaStreamSynchronize(e->compute), "cudaStreamSynchronize");
     return 0;
   });
 }

@@ -62,6 +62,14 @@ int choose_seg_rows(const std::vector<ThresholdPlan::Shape> &shapes, uint64_t re
 
 } // namespace
 
+int model_seg_rows(int elem_bytes, const std::vector<ThresholdPlan::Shape> &shapes, int wpc) {
+  const int occ = elem_bytes == 2 ? threshold_occupancy<uint16_t>(wpc)
+                                  : threshold_occupancy<uint32_t>(wpc);
+  if (occ < 1)
+    throw DeviceError("the threshold kernel does not fit on this device");
+  return choose_seg_rows(shapes, static_cast<uint64_t>(device_sm_count()) * occ * wpc);
+}
+
 void encode_arena_map(CUtensorMap *map, void *base, int elem_bytes, uint64_t pitch_elems,
                       uint64_t rows) {
   const cuuint64_t dims[2] = {pitch_elems, rows};

@@ -140,6 +140,7 @@ struct ServerSeries {
   std::vector<std::vector<Pixel>> pixels;
   std::vector<uint32_t> signal_counts;
   std::vector<int64_t> t_submit; // per frame number
+  int64_t t_close = 0;           // when the series was closed
   std::vector<double> lat_mask, lat_grouped, lat_spot;
   sf_counts counts{};
   uint64_t frames_done = 0, dropped = 0;
@@ -439,10 +440,14 @@ struct Server {
     const int64_t t = now_ns();
     std::lock_guard<std::mutex> g(se.m);
     se.counts = c;
+    // these spots were still open when the series was closed: closing is
+    // what finishes them, so their latency counts from the close (or from
+    // their last frame's submit, were that later)
     for (const Spot &s : sp) {
       const int64_t last = static_cast<int64_t>(s.bbox[5]) - 1 - se.first_frame;
       if (last >= 0 && last < static_cast<int64_t>(se.t_submit.size()))
-        se.lat_spot.push_back(1e-3 * static_cast<double>(t - se.t_submit[last]));
+        se.lat_spot.push_back(
+            1e-3 * static_cast<double>(t - std::max(se.t_close, se.t_submit[last])));
     }
     if (!sp.empty())
       se.spots.push_back(std::move(sp));
@@ -453,6 +458,8 @@ struct Server {
   void stop(ServerSeries &se) {
     {
       std::lock_guard<std::mutex> g(se.m);
+      if (!se.closing)
+        se.t_close = now_ns();
       se.closing = true;
       se.cv.notify_all();
     }

@@ -21,6 +21,7 @@ constexpr int kRunEvents = 4;
 
 struct Engine {
   std::unique_ptr<ThresholdPlan> plan;
+  bool tuned_from_cache = false; // the plan's tuning came from the tuner file
   // Streams: uploads on `copy`; threshold and placement on `compute`; the
   // grouping, when enabled, on `group`, so that the next run's threshold
   // overlaps this run's grouping. Per slot, events order the upload before

@@ -169,4 +169,35 @@ private:
   uint32_t *block_sums_ = nullptr;
 };
 
+// The cost model's task height (plan.cu) for these shapes at `wpc` warps per
+// block and as many blocks per SM as fit.
+int model_seg_rows(int elem_bytes, const std::vector<ThresholdPlan::Shape> &shapes, int wpc);
+
+// The autotuner (tune.cu). An entry is what a search measured best for one
+// frame shape on one kind of device: frames per launch, warps per block, the
+// task height as a ratio to the cost model's, and the time per frame.
+struct TuneEntry {
+  int frames = 16;
+  int warps_per_block = 4;
+  double seg_ratio = 1.0;
+  double us_per_frame = 0.0;
+};
+struct TuneOptions {
+  int min_frames = 8, max_frames = 32, steps = 4;
+  bool grouping = true, use_cache = true;
+  uint64_t hbm_budget = 0; // 0: half the free device memory
+  const char *cache_path = nullptr;
+};
+struct TuneResult {
+  TuneEntry entry;
+  bool from_cache = false;
+  int candidates = 0;
+};
+std::string tune_cache_path(const char *given);
+bool tune_lookup(int elem_bytes, int height, int width, const char *cache_path, TuneEntry *out);
+int tune_seg_rows(int elem_bytes, const std::vector<ThresholdPlan::Shape> &shapes, int wpc,
+                  double ratio);
+TuneResult tune_search(int elem_bytes, int height, int width, const void *const *sample,
+                       int nsample, const TuneOptions &options);
+
 } // namespace sf

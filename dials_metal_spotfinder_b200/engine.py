@@ -9,12 +9,16 @@ import ctypes
 
 import numpy as np
 
-from ._lib import (COUNT_NAMES, PIXEL, SIGNAL_PIXEL, SPOT, EngineConfig, GroupOptions, lib,
-                   raise_for, require_device)
+from ._lib import (COUNT_NAMES, PIXEL, SIGNAL_PIXEL, SPOT, EngineConfig, GroupOptions,
+                   TuneResult, lib, raise_for, require_device)
 
 
 class Engine:
-    def __init__(self, shapes, dtype=np.uint16, slots=1, seg_rows=0, warps_per_block=4,
+    """seg_rows and warps_per_block 0 (the default): the tuner file's choice
+    for this frame shape on this device (see tune.py), else the cost model's
+    task height and 4 warps per block."""
+
+    def __init__(self, shapes, dtype=np.uint16, slots=1, seg_rows=0, warps_per_block=0,
                  blocks_per_sm=0):
         require_device()
         self.dtype = np.dtype(dtype)
@@ -57,6 +61,16 @@ class Engine:
         keys = ("seg_rows", "warps_per_block", "grid_blocks", "tasks", "slots",
                 "device_bytes", "pitch", "capacity")
         return dict(zip(keys, list(out)))
+
+    def tuning(self) -> dict:
+        """frames_per_launch, warps_per_block, seg_rows and from_cache (the
+        tuning came from the tuner file)."""
+        out = TuneResult()
+        raise_for(lib.sf_engine_tuning(self._h, ctypes.byref(out)), "sf_engine_tuning")
+        d = out.as_dict()
+        d["from_cache"] = bool(d["from_cache"])
+        return {k: d[k] for k in ("frames_per_launch", "warps_per_block", "seg_rows",
+                                  "from_cache")}
 
     def upload(self, slot: int, frame: int, image: np.ndarray) -> None:
         """Asynchronous host-to-device copy; keep `image` alive (and unchanged)
@@ -126,21 +140,49 @@ class Engine:
         raise_for(lib.sf_engine_counts(self._h, slot, out.ctypes.data), "counts")
         return out
 
-    def signal_status(self, slot: int, frame: int):
+    def signal_status(self, slot: int, frame: int, out: np.ndarray | None = None):
+        """(status, list) of one frame of the slot's last run. With `out` (a
+        SIGNAL_PIXEL array of at least the frame's capacity, height * width *
+        itemsize / 16 records; page-locked copies fastest) the list is copied
+        into it and a view of the filled part returned."""
         h, w = self.shapes[frame]
         cap = max(h * w * self.dtype.itemsize // 16, 1)
-        out = np.empty(cap, SIGNAL_PIXEL)
+        given = out is not None
+        if given:
+            if out.dtype != SIGNAL_PIXEL or out.ndim != 1 or not out.flags.c_contiguous \
+                    or len(out) < cap:
+                raise ValueError("out must be a contiguous SIGNAL_PIXEL array of the "
+                                 "frame's capacity")
+        else:
+            out = np.empty(cap, SIGNAL_PIXEL)
         found = ctypes.c_size_t(0)
-        status = lib.sf_engine_signal(self._h, slot, frame, out.ctypes.data, cap,
+        status = lib.sf_engine_signal(self._h, slot, frame, out.ctypes.data, len(out),
                                       ctypes.byref(found))
         if status == -3:
             raise_for(status, "signal")
         if status != 0:
             return status, np.zeros(0, SIGNAL_PIXEL)
-        return 0, out[: found.value].copy()
+        return 0, out[: found.value] if given else out[: found.value].copy()
 
-    def signal(self, slot: int, frame: int) -> np.ndarray:
-        status, sig = self.signal_status(slot, frame)
+    def signals(self, slot: int, out: np.ndarray | None = None):
+        """Every frame's list of the slot's last run: (lists, counts), the
+        lists back to back in frame order in `out` (or a new array) and
+        returned as views. Overflow if a frame overflowed or they do not
+        fit."""
+        counts = np.zeros(self.nframes, np.uint32)
+        if out is None:
+            cap = sum(max(h * w * self.dtype.itemsize // 16, 1) for h, w in self.shapes)
+            out = np.empty(cap, SIGNAL_PIXEL)
+        elif out.dtype != SIGNAL_PIXEL or out.ndim != 1 or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous SIGNAL_PIXEL array")
+        raise_for(lib.sf_engine_signals(self._h, slot, out.ctypes.data, len(out),
+                                        counts.ctypes.data), "signals")
+        ends = np.cumsum(counts.astype(np.int64))
+        starts = ends - counts
+        return [out[a:b] for a, b in zip(starts, ends)], counts
+
+    def signal(self, slot: int, frame: int, out: np.ndarray | None = None) -> np.ndarray:
+        status, sig = self.signal_status(slot, frame, out)
         raise_for(status, "signal")
         return sig
 

@@ -3,8 +3,9 @@ one device, admitted by device-memory budget, frames submitted as detector
 chunks and decoded, thresholded and grouped on the device as they arrive,
 concurrent series overlapping on the device. Also a driver that replays
 streams at fixed frame rates and reports latency percentiles, and the plain
-per-frame form (host decode, sf_find per frame, labeller per frame) run on
-the same streams for comparison."""
+per-frame GPU form (worker threads decoding on the host and calling sf_find
+per frame, a labeller fed in frame order) run on the same streams for
+comparison."""
 
 from __future__ import annotations
 
@@ -176,59 +177,105 @@ def drive(streams, hbm_budget=0, slots=3, use_graph=True):
     return out
 
 
-def drive_plain(streams):
-    """The plain per-frame form on the same streams: per frame, host decode,
-    sf_find_u16 (upload, threshold, copy back) and a device labeller add, on
-    one host thread per stream. Latencies in ms from each frame's due time."""
+def drive_plain(streams, workers: int | None = None, give_up_s: float = 5.0):
+    """The plain per-frame GPU form on the same streams, threaded the way the
+    reference CLI runs it with -gpu (src/find_spots.cc:472-591): per stream,
+    `workers` threads take frames as they fall due, each decoding its chunk
+    on the host and calling sf_find_u16 (the reference's gpu::find: upload,
+    threshold, list back); one thread per stream adds the lists to a device
+    labeller in frame order. A frame not started within `give_up_s` of its
+    due time is dropped (the run stays bounded when the form cannot keep
+    up). Latencies in ms from due times: frame-to-mask when the frame's list
+    is on the host, frame-to-spot when the labeller has emitted the spot,
+    from its last frame's due time."""
+    import os
+    import queue
+
     from . import chunk as C
     from . import find
     from .labeller import Labeller
-    out = []
+    if workers is None:
+        workers = min(8, max(2, (os.cpu_count() or 4) // (2 * max(1, len(streams)))))
     t0 = time.perf_counter() + 0.05
     results = [None] * len(streams)
 
-    def consume(k):
+    def run_stream(k):
         s = streams[k]
         period = 1.0 / s.rate_hz
-        lab = Labeller(*s.shape, two_d=s.two_d)
-        mask, spot_lat = [], []
-        pending_due = []
-        backlog = 0
-        for i in range(s.frames):
-            due = t0 + i * period
-            while True:
-                now = time.perf_counter()
-                if now >= due:
-                    break
-                time.sleep(min(due - now, 0.0005))
-            img = C.decode(s.chunks[i % len(s.chunks)], s.shape, np.uint16, s.algorithm)
-            sig = find(img)
-            t_mask = time.perf_counter()
-            mask.append(t_mask - due)
-            before = lab.spots()
-            lab.add(i, sig)
-            after = lab.spots()
-            t_spot = time.perf_counter()
-            for sp in after[len(before):]:
-                last = int(sp["bbox"][5]) - 1
-                spot_lat.append(t_spot - (t0 + last * period))
-            pending_due.append(due)
-            backlog = max(backlog, int((time.perf_counter() - due) / period))
-        lab.finish()
-        lab.close()
-        results[k] = (mask, spot_lat, backlog)
+        jobs = queue.Queue()
+        done = {}
+        cv = threading.Condition()
+        mask = []
 
-    threads = [threading.Thread(target=consume, args=(k,)) for k in range(len(streams))]
+        def produce():
+            for i in range(s.frames):
+                due = t0 + i * period
+                while True:
+                    now = time.perf_counter()
+                    if now >= due:
+                        break
+                    time.sleep(min(due - now, 0.0005))
+                jobs.put(i)
+            for _ in range(workers):
+                jobs.put(None)
+
+        def work():
+            while True:
+                i = jobs.get()
+                if i is None:
+                    return
+                due = t0 + i * period
+                sig = None
+                if time.perf_counter() - due <= give_up_s:
+                    img = C.decode(s.chunks[i % len(s.chunks)], s.shape, np.uint16, s.algorithm)
+                    sig = find(img)
+                t = time.perf_counter()
+                with cv:
+                    done[i] = (sig, t)
+                    cv.notify_all()
+
+        lab = Labeller(*s.shape, two_d=s.two_d)
+        emitted = []  # (spots emitted so far, time) after each add
+        dropped = 0
+        threads = [threading.Thread(target=produce)]
+        threads += [threading.Thread(target=work) for _ in range(workers)]
+        for t in threads:
+            t.start()
+        for i in range(s.frames):
+            with cv:
+                cv.wait_for(lambda: i in done)
+                sig, t_mask = done.pop(i)
+            if sig is None:
+                dropped += 1
+                continue
+            mask.append(t_mask - (t0 + i * period))
+            lab.add(i, sig)
+            emitted.append((int(lib.sf_labeller_nspots(lab._h)), time.perf_counter()))
+        for t in threads:
+            t.join()
+        spots = lab.spots()
+        lab.close()
+        spot_lat, j = [], 0
+        for n_after, t in emitted:
+            while j < min(n_after, len(spots)):
+                last = int(spots[j]["bbox"][5]) - 1
+                spot_lat.append(t - (t0 + last * period))
+                j += 1
+        results[k] = (mask, spot_lat, dropped)
+
+    threads = [threading.Thread(target=run_stream, args=(k,)) for k in range(len(streams))]
     for t in threads:
         t.start()
     for t in threads:
         t.join()
     wall = time.perf_counter() - t0
+    out = []
     for k, s in enumerate(streams):
-        mask, spot_lat, backlog = results[k]
+        mask, spot_lat, dropped = results[k]
         out.append({
             "shape": list(s.shape), "rate_hz": s.rate_hz, "frames": s.frames,
-            "sustained_fps": s.frames / wall, "max_backlog_frames": backlog,
+            "workers": workers, "dropped": dropped,
+            "sustained_fps": (s.frames - dropped) / wall,
             "frame_to_mask_ms": {k2: (v * 1e3 if v is not None else None)
                                  for k2, v in percentiles(mask).items()},
             "frame_to_spot_ms": {k2: (v * 1e3 if v is not None else None)

@@ -234,11 +234,15 @@ SF_API int sf_refl_write(const char *path, const sf_spot *spots, size_t nspots,
 typedef struct sf_engine sf_engine;
 
 typedef struct sf_engine_config {
-  int32_t seg_rows;        /* output rows per warp task; 0 = the cost model's choice */
-  int32_t warps_per_block; /* 1, 2 or 4; 0 = 4 */
+  int32_t seg_rows;        /* output rows per warp task; 0 = tuned or the cost model's */
+  int32_t warps_per_block; /* 1, 2 or 4; 0 = tuned, else 4 */
   int32_t blocks_per_sm;   /* 0 = as many as fit */
   int32_t slots;           /* device arenas; 0 = 1 */
 } sf_engine_config;
+/* With seg_rows and warps_per_block both 0 (or no config), an engine whose
+ * frames all have one shape reads the tuner file (sf_tune) for that shape on
+ * this kind of device and uses its warps per block and task height; without
+ * an entry it uses the cost model and 4 warps per block. */
 
 SF_API int sf_engine_create(int elem_bytes, int nframes, const int32_t *heights,
                             const int32_t *widths, const sf_engine_config *config,
@@ -287,6 +291,14 @@ SF_API int sf_engine_counts(sf_engine *engine, int slot, uint32_t *counts);
  * including -2 beyond the list capacity. */
 SF_API int sf_engine_signal(sf_engine *engine, int slot, int frame, sf_signal_pixel *out,
                             size_t capacity, size_t *found);
+/* Every frame's list of the slot's last run, back to back in frame order
+ * into `out` (`capacity` records), with each frame's count in counts[frame]
+ * (nframes entries): one count read and one copy per frame, waiting once.
+ * -2 (counts still filled) if a frame overflowed its list or the lists do
+ * not fit in `capacity`. The per-frame gpu::find of the reference
+ * (src/dext_gpu.hh:141-158) over a whole batch. */
+SF_API int sf_engine_signals(sf_engine *engine, int slot, sf_signal_pixel *out, size_t capacity,
+                             uint32_t *counts);
 /* CUDA events on the compute stream: record mark 0..15; elapsed ms between
  * two marks (waits for the later one). */
 SF_API int sf_engine_record(sf_engine *engine, int mark);
@@ -297,6 +309,45 @@ SF_API int sf_engine_elapsed(sf_engine *engine, int from, int to, float *ms);
  * placement ms and grouping ms, summed over the runs since. */
 SF_API int sf_engine_profile(sf_engine *engine, int on);
 SF_API int sf_engine_stage_totals(sf_engine *engine, double out4[4]);
+
+/* ---- the autotuner ------------------------------------------------------ *
+ * A timed search for one frame shape on the current device: warps per block
+ * x threshold task height (threshold alone), then frames per launch
+ * (threshold + placement + 3D grouping, two slots, as the engine overlaps
+ * them), on the caller's sample frames (host, row-major, cycled into the
+ * batches), with CUDA events. The best tuple is appended to a tuner file,
+ * keyed by pixel type, shape, SM count and device name; engines created
+ * without explicit tuning read it. Results never depend on the tuning, only
+ * the time does. The reference chooses its stage windows by measurement
+ * the same way (src/dext_gpu.cc:18-37, tests/bench_dext_gpu.cc:242-337). */
+typedef struct sf_tune_options {
+  int32_t min_frames;   /* frames per launch tried: 0 = 8 */
+  int32_t max_frames;   /* 0 = 32 */
+  int32_t steps;        /* timed runs per candidate; 0 = 4 */
+  int32_t grouping;     /* time the step with 3D grouping (1) or threshold only */
+  int32_t use_cache;    /* return the tuner file's entry if there is one */
+  int32_t reserved;
+  uint64_t hbm_budget;  /* device bytes a candidate may use; 0 = half the free */
+  const char *cache_path; /* NULL: $SPOTFINDER_TUNE_CACHE, else
+                             $XDG_CACHE_HOME or ~/.cache /spotfinder_b200/tune.txt */
+} sf_tune_options;
+
+typedef struct sf_tune_result {
+  int32_t frames_per_launch;
+  int32_t warps_per_block;
+  int32_t seg_rows;       /* for frames_per_launch frames */
+  int32_t from_cache;     /* 1: read from the tuner file, no search */
+  int32_t candidates;     /* configurations timed */
+  int32_t reserved;
+  double seg_ratio;       /* task height / the cost model's */
+  double us_per_frame;    /* the chosen tuple's measured time per frame */
+} sf_tune_result;
+
+SF_API int sf_tune(int elem_bytes, int height, int width, const void *const *sample_frames,
+                   int nsample, const sf_tune_options *options, sf_tune_result *out);
+/* The tuning an engine runs with: frames per launch, warps per block, task
+ * height, and whether they came from the tuner file. */
+SF_API int sf_engine_tuning(sf_engine *engine, sf_tune_result *out);
 
 /* Grouping inside every run. The batch's frames of one shape form one
  * series (several shapes: several series, e.g. concurrent detectors or

@@ -34,6 +34,10 @@ def fake_engine(sf):
         def info(self):
             return {"seg_rows": 0, "slots": 2}
 
+        def tuning(self):
+            return {"frames_per_launch": len(self.shapes), "warps_per_block": 4,
+                    "seg_rows": 100, "from_cache": False}
+
         def upload(self, slot, frame, image):
             assert image.shape == self.shapes[frame]
 
@@ -104,7 +108,7 @@ def test_bench_line_has_the_contract_keys(monkeypatch):
                         lambda n: [np.zeros(bench.SHAPE, np.uint16) for _ in range(n)])
     monkeypatch.setattr(sys, "argv", ["bench.py", "--steps", "2", "--warmup", "3", "--no-cpu",
                                       "--serve-seconds", "0", "--no-4m", "--e2e-steps", "2",
-                                      "--pool", "2"])
+                                      "--pool", "2", "--no-tune", "--no-u32"])
     out = io.StringIO()
     with contextlib.redirect_stdout(out):
         bench.main()

@@ -180,3 +180,23 @@ def test_results_into_pinned_arrays(gpu_lib):
         pb.close()
     assert np.concatenate(spots).tobytes() == ref_spots.tobytes()
     assert np.concatenate(pixels).tobytes() == ref_pixels.tobytes()
+
+
+def test_batch_list_read_equals_per_frame_reads(gpu_lib):
+    """signals(): every frame's list in one call, back to back, equal to the
+    per-frame reads; a too-small array is refused with the counts filled."""
+    import dials_metal_spotfinder_b200 as sf
+    from dials_metal_spotfinder_b200.engine import Engine
+    shapes = [(300, 500), (64, 90), (531, 233)]
+    frames = frames_for(shapes, 9)
+    with Engine(shapes, np.uint16) as eng:
+        for f, img in enumerate(frames):
+            eng.upload(0, f, img)
+        eng.run(0)
+        lists, counts = eng.signals(0)
+        for f, img in enumerate(frames):
+            assert lists[f].tobytes() == eng.signal(0, f).tobytes()
+            assert lists[f].tobytes() == O.dext(img)[1].tobytes()
+            assert counts[f] == len(lists[f])
+        with pytest.raises(sf.Overflow):
+            eng.signals(0, out=np.zeros(int(counts.sum()) - 1, sf.SIGNAL_PIXEL))
