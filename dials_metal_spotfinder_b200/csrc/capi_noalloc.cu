@@ -49,7 +49,7 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 namespace {
 
 constexpr int kMaxDevices = 64;
-constexpr int kWarpsPerBlock = 4;
+constexpr int kWarpsPerBlock = 2;
 constexpr int kBlocksPerSm = 2; // bounds the staging pool: one open chunk per warp
 
 std::mutex g_lock;
@@ -118,7 +118,7 @@ Layout plan_layout(uint64_t height, uint64_t width) {
                                              static_cast<uint64_t>(L.max_blocks));
   const uint64_t warps = blocks * kWarpsPerBlock;
   const uint64_t chunks =
-      (cap + (kChunkRecords - kStripOut) - 1) / (kChunkRecords - kStripOut) + warps + 1;
+      (cap + (kChunkRecords - kMaxStaged) - 1) / (kChunkRecords - kMaxStaged) + warps + 1;
   const uint64_t pool_records = chunks * kChunkRecords;
   const uint64_t place_blocks = (L.ntiles + kPlaceTiles - 1) / kPlaceTiles;
   L.arena_bytes = L.pitch * L.rows * sizeof(uint16_t);

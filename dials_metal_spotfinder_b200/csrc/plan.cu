@@ -164,7 +164,7 @@ ThresholdPlan::ThresholdPlan(int elem_bytes, const std::vector<Shape> &shapes,
   grid_blocks_ = static_cast<int>(std::min<uint64_t>((ntasks_ + wpc - 1) / wpc, max_blocks_));
   const uint64_t warps = static_cast<uint64_t>(grid_blocks_) * wpc;
   const uint64_t chunks =
-      (total_capacity_ + (kChunkRecords - kStripOut) - 1) / (kChunkRecords - kStripOut) +
+      (total_capacity_ + (kChunkRecords - kMaxStaged) - 1) / (kChunkRecords - kMaxStaged) +
       warps + 1;
   const uint64_t pool_records = chunks * kChunkRecords;
   if (pool_records >= 0xffffffffull - kChunkRecords)

@@ -36,6 +36,10 @@ constexpr int kRingRows = 24;              // rows of a strip held in smem
 constexpr int kBoxRows = 4;                // rows per TMA box
 constexpr int kRingStages = kRingRows / kBoxRows;
 constexpr uint32_t kChunkRecords = 1024;   // staging pool allocation unit
+// The most records a warp stages at once (two output rows of a strip); a
+// staging chunk is abandoned when that many might not fit, so each chunk
+// wastes fewer than this.
+constexpr uint32_t kMaxStaged = 2 * kStripOut;
 
 // Pixel-type traits. The window sums of the reference are accumulated in
 // accumulator_t<T> (uint32 for 16-bit pixels, uint64 for 32-bit) and tested

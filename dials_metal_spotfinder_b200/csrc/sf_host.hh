@@ -84,7 +84,7 @@ int device_sm_count();
 // Launch geometry of the threshold for one batch shape.
 struct PlanTuning {
   int seg_rows = 0;        // output rows per task; 0 picks by frame count
-  int warps_per_block = 4; // 1, 2 or 4
+  int warps_per_block = 2; // 1, 2 or 4
   int blocks_per_sm = 0;   // 0: as many as fit
 };
 
@@ -178,7 +178,7 @@ int model_seg_rows(int elem_bytes, const std::vector<ThresholdPlan::Shape> &shap
 // task height as a ratio to the cost model's, and the time per frame.
 struct TuneEntry {
   int frames = 16;
-  int warps_per_block = 4;
+  int warps_per_block = 2;
   double seg_ratio = 1.0;
   double us_per_frame = 0.0;
 };

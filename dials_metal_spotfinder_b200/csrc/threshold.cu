@@ -131,14 +131,17 @@ __device__ __forceinline__ uint32_t dispersion_bits(const uint32_t (&hs)[8],
 }
 
 // The same when every window holds 49 pixels: m, m - 1 and the square root
-// are constants (sq49 = sqrt_term(49)).
+// are constants (sq49 = sqrt_term(49)). s * 48 is formed as 8 * (s * 6):
+// scaling by a power of two is exact and commutes with rounding, so
+// fl(s * 48) = 8 fl(s * 6), and t3 - fl(s * 48) is one fused operation on
+// the already rounded fl(s * 6), which the right side needs anyway.
 __device__ __forceinline__ uint32_t dispersion_bits49(const uint32_t (&hs)[8],
                                                       const uint32_t (&hq)[8], float sq49) {
   const float2 magic = make_float2(-8388608.0f, -8388608.0f);
   const float2 neg1 = make_float2(-1.0f, -1.0f);
+  const float2 neg8 = make_float2(-8.0f, -8.0f);
   const float2 six = make_float2(6.0f, 6.0f);
   const float2 c49 = make_float2(49.0f, 49.0f);
-  const float2 c48 = make_float2(48.0f, 48.0f);
   const float2 R = make_float2(sq49, sq49);
   uint32_t bits = 0;
 #pragma unroll
@@ -150,9 +153,9 @@ __device__ __forceinline__ uint32_t dispersion_bits49(const uint32_t (&hs)[8],
     const float2 t1 = __fmul2_rn(c49, Q);
     const float2 t2 = __fmul2_rn(S, S);
     const float2 t3 = __ffma2_rn(t2, neg1, t1);
-    const float2 t5 = __fmul2_rn(S, c48);
-    const float2 lhs = __ffma2_rn(t5, neg1, t3);
-    const float2 rhs = __fmul2_rn(__fmul2_rn(S, six), R);
+    const float2 u = __fmul2_rn(S, six);                      // s * 6
+    const float2 lhs = __ffma2_rn(u, neg8, t3);               // t3 - 8 (s * 6)
+    const float2 rhs = __fmul2_rn(u, R);
     const float2 d = __ffma2_rn(lhs, neg1, rhs);
     bits = push_sign(bits, d.y);
     bits = push_sign(bits, d.x);
@@ -214,15 +217,19 @@ template <> struct LaneRow<uint16_t> {
     p[4] = v.z & 0xffffu; p[5] = v.z >> 16;
     p[6] = v.w & 0xffffu; p[7] = v.w >> 16;
   }
-  // Nonzero iff a pixel is 0xfffe or 0xffff: such a half is all ones once
-  // its low bit is set, so its complement is a zero half, which the borrow
-  // of a 16-bit subtract finds.
+  // Nonzero iff a pixel is 0xfffe or 0xffff (masked): the halfword maxima
+  // of the four words, compared with 0xfffe per half.
   __device__ __forceinline__ uint32_t any_masked() const {
-    auto z = [](uint32_t w) {
-      const uint32_t b = ~(w | 0x00010001u);
-      return (b - 0x00010001u) & ~b & 0x80008000u;
-    };
-    return z(v.x) | z(v.y) | z(v.z) | z(v.w);
+    const uint32_t m = __vmaxu2(__vmaxu2(v.x, v.y), __vmaxu2(v.z, v.w));
+    return __vcmpgeu2(m, 0xfffefffeu);
+  }
+  // Bit k set where pixel k is masked.
+  __device__ __forceinline__ uint32_t masked_bits() const {
+    const uint32_t x = (__vcmpgeu2(v.x, 0xfffefffeu) & 0x00010001u) |
+                       ((__vcmpgeu2(v.y, 0xfffefffeu) & 0x00010001u) << 2) |
+                       ((__vcmpgeu2(v.z, 0xfffefffeu) & 0x00010001u) << 4) |
+                       ((__vcmpgeu2(v.w, 0xfffefffeu) & 0x00010001u) << 6);
+    return (x | (x >> 15)) & 0xffu;
   }
 };
 
@@ -237,11 +244,13 @@ template <> struct LaneRow<uint32_t> {
     p[0] = a.x; p[1] = a.y; p[2] = a.z; p[3] = a.w;
     p[4] = b.x; p[5] = b.y; p[6] = b.z; p[7] = b.w;
   }
-  __device__ __forceinline__ uint32_t any_masked() const {
+  __device__ __forceinline__ uint32_t masked_bits() const {
     const uint32_t m = Traits<uint32_t>::kMasked;
-    return (a.x >= m) | (a.y >= m) | (a.z >= m) | (a.w >= m) | (b.x >= m) | (b.y >= m) |
-           (b.z >= m) | (b.w >= m);
+    return (a.x >= m ? 1u : 0u) | (a.y >= m ? 2u : 0u) | (a.z >= m ? 4u : 0u) |
+           (a.w >= m ? 8u : 0u) | (b.x >= m ? 16u : 0u) | (b.y >= m ? 32u : 0u) |
+           (b.z >= m ? 64u : 0u) | (b.w >= m ? 128u : 0u);
   }
+  __device__ __forceinline__ uint32_t any_masked() const { return masked_bits(); }
 };
 
 template <typename T>
@@ -327,34 +336,50 @@ __device__ __forceinline__ int back_slot(int slot, int back) {
   return s < 0 ? s + kRingRows : s;
 }
 
-// 16 warps per SM for 16-bit pixels (12 KB rings); 32-bit rings are twice
-// the size, so 8 warps fit and the registers can be spent instead.
+// Warps per SM the shared memory holds: a warp's ring, the 11-row sums of
+// two rows and their candidate list (15 KB for 16-bit pixels, 30 KB for
+// 32-bit).
+template <typename T> constexpr int kWarpsPerSm = sizeof(T) == 2 ? 14 : 7;
+
+// The rows before a task's first are read as zeros: 16 rows, the farthest
+// back any row's sums reach (the 11-row window's leaving row, 16 above).
+constexpr int kPreRows = 16;
+
+// Per-warp shared memory (the square-root table is static).
+template <typename T> struct WarpSmem {
+  using A = typename Traits<T>::Acc;
+  static constexpr uint32_t kRing = kStripCols * sizeof(T) * kRingRows;
+  static constexpr uint32_t kWin = 2 * kStripCols * sizeof(A);
+  static constexpr uint32_t kBars = kRingStages * sizeof(uint64_t);
+  static constexpr uint32_t kCand = 2 * kStripOut * sizeof(uint16_t);
+  static constexpr uint32_t kTotal = kRing + kWin + kBars + kCand;
+};
+
 template <typename T, int WPC>
-__global__ void __launch_bounds__(WPC * 32, (sizeof(T) == 2 ? 16 : 8) / WPC)
+__global__ void __launch_bounds__(WPC * 32, (kWarpsPerSm<T> / WPC) > 0 ? kWarpsPerSm<T> / WPC : 1)
     threshold_kernel(const __grid_constant__ CUtensorMap arena, ThresholdArgs args) {
   using Tr = Traits<T>;
   using A = typename Tr::Acc;
   using Rl = typename Real<T>::type;
+  using Sm = WarpSmem<T>;
   constexpr uint32_t kRowBytes = kStripCols * sizeof(T);
   constexpr uint32_t kBoxBytes = kRowBytes * kBoxRows;
   constexpr A C7 = A(1) << Tr::kShift7;   // one valid pixel's count in a 7 x 7 sum
   constexpr A C11 = A(1) << Tr::kShift11; // ... in an 11 x 11 sum
-  constexpr int kWarmup = 21;             // rows before every stage is live
+  constexpr int kVecs = kStripCols * sizeof(T) / (32 * 16); // 16-byte words per lane per row
 
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   __shared__ Rl sqrt_tab[64];
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  // Per warp: the ring, the 11-row vertical sums of one row (for the
-  // candidates), the stage barriers and the candidate column list.
   unsigned char *at = smem_raw;
-  T *ring = reinterpret_cast<T *>(at + warp * (kRowBytes * kRingRows));
-  at += WPC * (kRowBytes * kRingRows);
-  A *win11 = reinterpret_cast<A *>(at) + warp * kStripCols;
-  at += WPC * kStripCols * sizeof(A);
-  uint64_t *bars = reinterpret_cast<uint64_t *>(at) + warp * kRingStages;
-  at += WPC * kRingStages * sizeof(uint64_t);
-  uint8_t *cand_col = at + warp * kStripCols;
+  T *ring = reinterpret_cast<T *>(at + warp * Sm::kRing);
+  at += WPC * Sm::kRing;
+  A *win = reinterpret_cast<A *>(at + warp * Sm::kWin);
+  at += WPC * Sm::kWin;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(at + warp * Sm::kBars);
+  at += WPC * Sm::kBars;
+  uint16_t *cand = reinterpret_cast<uint16_t *>(at + warp * Sm::kCand);
 
   for (int m = threadIdx.x; m < 64; m += blockDim.x)
     sqrt_tab[m] = sqrt_term(m, Rl(0));
@@ -384,6 +409,7 @@ __global__ void __launch_bounds__(WPC * 32, (sizeof(T) == 2 ? 16 : 8) / WPC)
     const int rs = r0 - kHalo;       // first input row (frame coordinates)
     const int nrows = (r1 - r0) + 2 * kHalo;
     const int nboxes = (nrows + kBoxRows - 1) / kBoxRows;
+    const int nrows2 = (nrows + 1) & ~1; // rows are taken in pairs
     const int32_t tma_x = strip * kStripOut;
     const int64_t tma_y0 = fd.row0 + rs;
 
@@ -397,9 +423,26 @@ __global__ void __launch_bounds__(WPC * 32, (sizeof(T) == 2 ? 16 : 8) / WPC)
         outmask |= 1u << k;
     }
 
+    // The kPreRows rows above the task read as valid zeros, and every
+    // running sum and history starts as if they had been processed (7 and
+    // 11 valid zeros per column; nothing masked, dispersed, kept or a
+    // candidate), so the row body needs no warm-up branches. What those rows
+    // feed is flushed out before any output row reads it: an output row's
+    // windows reach 10 rows up, and the first output row is the task's
+    // 11th. They live in the ring slots of rows -16 .. -1, which no TMA box
+    // writes before they are last read.
+#pragma unroll 1
+    for (int i = 0; i < kPreRows; i++) {
+      uint4 *row = reinterpret_cast<uint4 *>(ring + (kRingRows - kPreRows + i) * kStripCols);
+#pragma unroll
+      for (int v = 0; v < kVecs; v++)
+        row[kVecs * lane + v] = make_uint4(0, 0, 0, 0);
+    }
+    fence_proxy_async_smem(); // these writes before any later TMA write of the slots
+    __syncwarp();
+
     // Prologue: the first two boxes.
     if (lane == 0) {
-      fence_proxy_async_smem();
       for (int b = 0; b < 2 && b < nboxes; b++) {
         const int st = b % kRingStages;
         mbar_expect_tx(&bars[st], kBoxBytes);
@@ -411,221 +454,305 @@ __global__ void __launch_bounds__(WPC * 32, (sizeof(T) == 2 ? 16 : 8) / WPC)
     A vs[8], vq[8], vg[8];
 #pragma unroll
     for (int k = 0; k < 8; k++) {
-      vs[k] = 0; vq[k] = 0; vg[k] = 0;
+      vs[k] = 7 * C7;
+      vq[k] = 0;
+      vg[k] = 11 * C11;
     }
-    uint64_t hist_mk = 0; // masked bits, rows r .. r-7
-    uint64_t hist_s0 = 0; // dispersion bits, rows a .. a-4 (a = r-3)
-    uint64_t gv_lo = 0;   // valid-and-not-eroded bits, rows b .. b-7 (b = r-5)
-    uint32_t gv_hi = 0;   //   rows b-8 .. b-11
-    uint64_t hist_cs = 0; // candidate-region bits, rows b .. b-5
-    uint32_t dirty = 0;   // warp-uniform: bit i = row r-i holds a masked pixel
-    uint32_t gdirty = 0;  // warp-uniform: bit i = row b-i holds a non-g pixel
+    // Histories, newest row in the low byte (bit), as they stand before the
+    // pair of rows r, r+1 enters:
+    uint64_t hist_mk = 0;   // masked bits of rows r-1 .. r-8
+    uint32_t hist_s0 = 0;   // dispersion bits of rows r-4 .. r-7
+    uint64_t gv_lo = ~0ull; // valid-and-not-kept bits of rows r-6 .. r-13
+    uint32_t gv_hi = ~0u;   //   rows r-14 .. r-17
+    uint64_t hist_cs = 0;   // candidate bits of rows r-6 .. r-13
+    uint32_t dirty = 0;     // warp-uniform: bit i = row r-1-i holds a masked pixel
+    uint32_t gdirty = 0;    // warp-uniform: bit i = row r-6-i holds a non-g pixel
 
     auto row_at = [&](int slot) { return ring + slot * kStripCols; };
 
-    // One input row: `rr` rows into the task, in ring slot `slot`. With
-    // `steady`, rr >= kWarmup and every stage runs unconditionally.
-    auto process_row = [&](int rr, int slot, auto steady_tag) {
-      constexpr bool steady = decltype(steady_tag)::value;
-
-      // ---- row r enters: masked bits -----------------------------------
-      LaneRow<T> raw;
-      raw.load(row_at(slot), lane);
-      uint32_t p[8];
-      raw.unpack(p);
-      uint32_t mk = 0;
-      const bool rdirty = __any_sync(kFull, raw.any_masked() != 0);
-      if (rdirty) {
-#pragma unroll
-        for (int k = 0; k < 8; k++)
-          mk |= (p[k] >= Tr::kMasked ? 1u : 0u) << k;
+    // Rows r = rr and r+1 of the task (ring slots `slot`, slot+1) enter.
+    // Row r's sums are completed before row r+1's; the stages of the two
+    // rows are otherwise independent, which gives the scheduler two rows of
+    // work to interleave.
+    auto process_pair = [&](int rr, int slot) {
+      // ---- loads, masks, and the pair's warp-wide flags -----------------
+      LaneRow<T> nA, nB, lA, lB;
+      nA.load(row_at(slot), lane);
+      nB.load(row_at(slot + 1), lane);
+      lA.load(row_at(back_slot(slot, 7)), lane);
+      lB.load(row_at(back_slot(slot, 6)), lane);
+      // candidates: rows c = r-10 and c+1, when they are output rows
+      const bool emitA = rr >= 2 * kHalo && rr < nrows;
+      const bool emitB = rr + 1 >= 2 * kHalo && rr + 1 < nrows;
+      const uint32_t csA = static_cast<uint32_t>(hist_cs >> 32) & (emitA ? outmask : 0u);
+      const uint32_t csB = static_cast<uint32_t>(hist_cs >> 24) & (emitB ? outmask : 0u);
+      const uint32_t flags = __reduce_or_sync(
+          kFull, (nA.any_masked() ? 1u : 0u) | (nB.any_masked() ? 2u : 0u) |
+                     ((csA | csB) ? 4u : 0u));
+      uint32_t mkA = 0, mkB = 0;
+      if (flags & 3u) {
+        mkA = nA.masked_bits();
+        mkB = nB.masked_bits();
       }
-      dirty = (dirty << 1) | (rdirty ? 1u : 0u);
-      hist_mk = (hist_mk << 8) | mk;
 
-      // ---- 7-row sums: + row r, - row r-7 --------------------------------
-      if (steady || rr >= 7) {
-        uint32_t q[8];
-        load_pixels<T>(row_at(back_slot(slot, 7)), lane, q);
+      // ---- 7-row sums: + rows r, r+1, - rows r-7, r-6 ------------------
+      uint32_t p[8], q[8];
+      A vsA[8], vqA[8];
+      nA.unpack(p);
+      lA.unpack(q);
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
-          const A d = static_cast<A>(p[k]) - static_cast<A>(q[k]);
-          vs[k] += d;
-          vq[k] += d * (static_cast<A>(p[k]) + static_cast<A>(q[k]));
-        }
-        if (dirty & 0x81u) {
-          const uint32_t mk7 = static_cast<uint32_t>(hist_mk >> 56) & 0xffu;
-          if (mk | mk7) {
+      for (int k = 0; k < 8; k++) {
+        const A d = static_cast<A>(p[k]) - static_cast<A>(q[k]);
+        vsA[k] = vs[k] + d;
+        vqA[k] = vq[k] + d * (static_cast<A>(p[k]) + static_cast<A>(q[k]));
+      }
+      if ((flags & 1u) | (dirty & 0x40u)) {
+        const uint32_t mk7 = static_cast<uint32_t>(hist_mk >> 48) & 0xffu; // row r-7
+        if (mkA | mk7) {
 #pragma unroll
-            for (int k = 0; k < 8; k++) {
-              if ((mk >> k) & 1u) {
-                vs[k] -= static_cast<A>(p[k]) + C7;
-                vq[k] -= static_cast<A>(p[k]) * static_cast<A>(p[k]);
-              }
-              if ((mk7 >> k) & 1u) {
-                vs[k] += static_cast<A>(q[k]) + C7;
-                vq[k] += static_cast<A>(q[k]) * static_cast<A>(q[k]);
-              }
+          for (int k = 0; k < 8; k++) {
+            if ((mkA >> k) & 1u) {
+              vsA[k] -= static_cast<A>(p[k]) + C7;
+              vqA[k] -= static_cast<A>(p[k]) * static_cast<A>(p[k]);
+            }
+            if ((mk7 >> k) & 1u) {
+              vsA[k] += static_cast<A>(q[k]) + C7;
+              vqA[k] += static_cast<A>(q[k]) * static_cast<A>(q[k]);
             }
           }
         }
-      } else {
+      }
+      nB.unpack(p);
+      lB.unpack(q);
 #pragma unroll
-        for (int k = 0; k < 8; k++) {
-          const A v = ((mk >> k) & 1u) ? A(0) : static_cast<A>(p[k]);
-          vs[k] += ((mk >> k) & 1u) ? A(0) : v + C7;
-          vq[k] += v * v;
+      for (int k = 0; k < 8; k++) {
+        const A d = static_cast<A>(p[k]) - static_cast<A>(q[k]);
+        vs[k] = vsA[k] + d;
+        vq[k] = vqA[k] + d * (static_cast<A>(p[k]) + static_cast<A>(q[k]));
+      }
+      if ((flags & 2u) | (dirty & 0x20u)) {
+        const uint32_t mk6 = static_cast<uint32_t>(hist_mk >> 40) & 0xffu; // row r-6
+        if (mkB | mk6) {
+#pragma unroll
+          for (int k = 0; k < 8; k++) {
+            if ((mkB >> k) & 1u) {
+              vs[k] -= static_cast<A>(p[k]) + C7;
+              vq[k] -= static_cast<A>(p[k]) * static_cast<A>(p[k]);
+            }
+            if ((mk6 >> k) & 1u) {
+              vs[k] += static_cast<A>(q[k]) + C7;
+              vq[k] += static_cast<A>(q[k]) * static_cast<A>(q[k]);
+            }
+          }
         }
       }
 
-      // ---- dispersion test at row a = r-3 ------------------------------
-      if (steady || rr >= 6) {
+      // ---- dispersion test at rows a = r-3 and a+1 ---------------------
+      // row a's window is rows r-6 .. r, row a+1's r-5 .. r+1
+      const bool wdA = ((dirty & 0x3fu) | (flags & 1u)) != 0;
+      const bool wdB = ((dirty & 0x1fu) | (flags & 3u)) != 0;
+      uint32_t s0A, s0B;
+      {
+        A hs[8], hq[8];
+        hsum<3>(vsA, hs);
+        hsum<3>(vqA, hq);
+        if constexpr (sizeof(T) == 2)
+          s0A = wdA ? dispersion_bits(hs, hq, sqrt_tab) : dispersion_bits49(hs, hq, sq49);
+        else
+          s0A = dispersion_bits(hs, hq, sqrt_tab);
+      }
+      {
         A hs[8], hq[8];
         hsum<3>(vs, hs);
         hsum<3>(vq, hq);
-        uint32_t bits;
-        if constexpr (sizeof(T) == 2) {
-          bits = (dirty & 0x7fu) ? dispersion_bits(hs, hq, sqrt_tab)
-                                 : dispersion_bits49(hs, hq, sq49);
-        } else {
-          bits = dispersion_bits(hs, hq, sqrt_tab);
-        }
-        const uint32_t s0 = (static_cast<uint32_t>(hist_mk >> 24) & 0xffu) | bits; // masked -> 1
-        hist_s0 = (hist_s0 << 8) | s0;
+        if constexpr (sizeof(T) == 2)
+          s0B = wdB ? dispersion_bits(hs, hq, sqrt_tab) : dispersion_bits49(hs, hq, sq49);
+        else
+          s0B = dispersion_bits(hs, hq, sqrt_tab);
       }
+      s0A |= static_cast<uint32_t>(hist_mk >> 16) & 0xffu; // masked -> 1 (row r-3)
+      s0B |= static_cast<uint32_t>(hist_mk >> 8) & 0xffu;  // row r-2
 
-      // ---- erode at row b = r-5, and the 11-row sums -------------------
-      if (steady || rr >= 10) {
-        const uint32_t v = static_cast<uint32_t>(hist_s0 & (hist_s0 >> 8) &
-                                                 (hist_s0 >> 16) & (hist_s0 >> 24) &
-                                                 (hist_s0 >> 32)) & 0xffu;
-        const uint32_t vl = shfl_up(v), vr = shfl_down(v);
-        const uint32_t w = (vl >> 6) | (v << 2) | (vr << 10);
-        const uint32_t hv = w & (w >> 1) & (w >> 2) & (w >> 3) & (w >> 4) & 0xffu;
-        const uint32_t mkb = static_cast<uint32_t>(hist_mk >> 40) & 0xffu;
-        const uint32_t s1 = hv | mkb;           // scr1, src/dext.cc:117-142
-        const uint32_t gv = ~s1 & 0xffu;        // valid and not kept
-        const uint32_t cs = s1 & ~mkb & 0xffu;  // kept and not masked
-        gv_hi = (gv_hi << 8) | static_cast<uint32_t>(gv_lo >> 56);
-        gv_lo = (gv_lo << 8) | gv;
-        hist_cs = (hist_cs << 8) | cs;
-        gdirty = (gdirty << 1) | (__any_sync(kFull, gv != 0xffu) ? 1u : 0u);
+      // ---- erode at rows b = r-5 and b+1 -------------------------------
+      // row b: dispersion rows r-7 .. r-3; row b+1: r-6 .. r-2. Both rows'
+      // bits travel in one word (row b in bits 0-7, b+1 in 16-23).
+      const uint32_t vA = s0A & hist_s0 & (hist_s0 >> 8) & (hist_s0 >> 16) & (hist_s0 >> 24);
+      const uint32_t vB = s0B & s0A & hist_s0 & (hist_s0 >> 8) & (hist_s0 >> 16);
+      hist_s0 = (hist_s0 << 16) | (s0A << 8) | s0B;
+      const uint32_t v2 = (vA & 0xffu) | ((vB & 0xffu) << 16);
+      const uint32_t vl = shfl_up(v2), vr = shfl_down(v2);
+      const uint32_t w2 = ((vl >> 6) & 0x00030003u) | (v2 << 2) | ((vr << 10) & 0x0c000c00u);
+      const uint32_t hv2 = w2 & (w2 >> 1) & (w2 >> 2) & (w2 >> 3) & (w2 >> 4) & 0x00ff00ffu;
+      const uint32_t mkb2 = (static_cast<uint32_t>(hist_mk >> 32) & 0xffu) |      // row r-5
+                            ((static_cast<uint32_t>(hist_mk >> 24) & 0xffu) << 16); // r-4
+      const uint32_t s1 = hv2 | mkb2;                 // scr1, src/dext.cc:117-142
+      const uint32_t gv2 = ~s1 & 0x00ff00ffu;         // valid and not kept
+      const uint32_t cs2 = s1 & ~mkb2 & 0x00ff00ffu;  // kept and not masked
+      const uint32_t gvA = gv2 & 0xffu, gvB = gv2 >> 16;
+      const uint32_t gflags =
+          __reduce_or_sync(kFull, (gvA != 0xffu ? 1u : 0u) | (gvB != 0xffu ? 2u : 0u));
 
-        uint32_t p5[8];
-        load_pixels<T>(row_at(back_slot(slot, 5)), lane, p5);
-        if (steady || rr >= kWarmup) {
-          uint32_t p16[8];
-          load_pixels<T>(row_at(back_slot(slot, 16)), lane, p16);
+      // ---- 11-row sums at rows b, b+1: + rows r-5, r-4, - rows r-16, r-15
+      const uint32_t ng16 = ~(gv_hi >> 16) & 0xffu; // row r-16
+      const uint32_t ng15 = ~(gv_hi >> 8) & 0xffu;  // row r-15
+      load_pixels<T>(row_at(back_slot(slot, 5)), lane, p);
+      load_pixels<T>(row_at(back_slot(slot, 16)), lane, q);
 #pragma unroll
-          for (int k = 0; k < 8; k++)
-            vg[k] += static_cast<A>(p5[k]) - static_cast<A>(p16[k]);
-          if (gdirty & ((1u << 11) | 1u)) {
-            const uint32_t ng5 = ~gv & 0xffu;
-            const uint32_t ng16 = ~(gv_hi >> 24) & 0xffu;
-            if (ng5 | ng16) {
+      for (int k = 0; k < 8; k++)
+        vg[k] += static_cast<A>(p[k]) - static_cast<A>(q[k]);
+      if ((gflags & 1u) | ((gdirty >> 10) & 1u)) {
+        const uint32_t ng5 = ~gvA & 0xffu;
+        if (ng5 | ng16) {
 #pragma unroll
-              for (int k = 0; k < 8; k++) {
-                if ((ng5 >> k) & 1u)
-                  vg[k] -= static_cast<A>(p5[k]) + C11;
-                if ((ng16 >> k) & 1u)
-                  vg[k] += static_cast<A>(p16[k]) + C11;
-              }
-            }
+          for (int k = 0; k < 8; k++) {
+            if ((ng5 >> k) & 1u)
+              vg[k] -= static_cast<A>(p[k]) + C11;
+            if ((ng16 >> k) & 1u)
+              vg[k] += static_cast<A>(q[k]) + C11;
           }
-        } else {
-#pragma unroll
-          for (int k = 0; k < 8; k++)
-            vg[k] += ((gv >> k) & 1u) ? static_cast<A>(p5[k]) + C11 : A(0);
         }
       }
-
-      // ---- Poisson test and emit at row c = r-10 -----------------------
-      if (steady || rr >= 2 * kHalo) {
-        const int c = rs + rr - kHalo; // frame row of the output
-        const uint32_t cs = static_cast<uint32_t>(hist_cs >> 40) & 0xffu & outmask;
-        if (__any_sync(kFull, cs != 0)) {
-          // The candidates are compacted one per lane before the Poisson
-          // test, so each pays for one division and one square root -- and
-          // for one 11-column sum of the vertical sums, read from shared
-          // memory -- instead of every lane paying for all eight columns.
+      A vgA[8];
 #pragma unroll
-          for (int k = 0; k < 8; k++)
-            win11[8 * lane + k] = vg[k];
-          // The candidate columns in ascending order: lane by lane, and
-          // within a lane by column.
-          const uint32_t cnt = __popc(cs);
-          uint32_t incl = cnt;
+      for (int k = 0; k < 8; k++)
+        vgA[k] = vg[k];
+      load_pixels<T>(row_at(back_slot(slot, 4)), lane, p);
+      load_pixels<T>(row_at(back_slot(slot, 15)), lane, q);
 #pragma unroll
-          for (int d = 1; d < 32; d <<= 1) {
-            const uint32_t t = __shfl_up_sync(kFull, incl, d);
-            if (lane >= d)
-              incl += t;
+      for (int k = 0; k < 8; k++)
+        vg[k] += static_cast<A>(p[k]) - static_cast<A>(q[k]);
+      if ((gflags & 2u) | ((gdirty >> 9) & 1u)) {
+        const uint32_t ng4 = ~gvB & 0xffu;
+        if (ng4 | ng15) {
+#pragma unroll
+          for (int k = 0; k < 8; k++) {
+            if ((ng4 >> k) & 1u)
+              vg[k] -= static_cast<A>(p[k]) + C11;
+            if ((ng15 >> k) & 1u)
+              vg[k] += static_cast<A>(q[k]) + C11;
           }
-          const uint32_t total = __shfl_sync(kFull, incl, 31);
-          {
-            uint32_t at = incl - cnt, left = cs;
-            while (left) {
-              cand_col[at++] = static_cast<uint8_t>(8 * lane + __ffs(left) - 1);
-              left &= left - 1;
-            }
-          }
-          __syncwarp();
+        }
+      }
 
-          // Room for every candidate in one chunk, so the tile's records
-          // are contiguous whatever the rounds below find.
-          if (chunk == kNoChunk || fill + total > kChunkRecords) {
-            uint32_t base = 0;
+      // ---- histories -----------------------------------------------------
+      gv_hi = (gv_hi << 16) | static_cast<uint32_t>(gv_lo >> 48);
+      gv_lo = (gv_lo << 16) | (gvA << 8) | gvB;
+      hist_cs = (hist_cs << 16) | ((cs2 & 0xffu) << 8) | (cs2 >> 16);
+      hist_mk = (hist_mk << 16) | (mkA << 8) | mkB;
+      dirty = (dirty << 2) | ((flags & 1u) << 1) | ((flags >> 1) & 1u);
+      gdirty = (gdirty << 2) | ((gflags & 1u) << 1) | ((gflags >> 1) & 1u);
+
+      // ---- Poisson test and emit at rows c = r-10 and c+1 ---------------
+      if (flags & 4u) {
+        // The 11-row sums of both rows, for the candidates' 11-column
+        // windows; then the candidates of both rows compacted one per lane
+        // (row c's first, each row's in column order), so that each pays
+        // for one division and one square root.
+        if constexpr (sizeof(A) == 4) {
+          uint4 *w0 = reinterpret_cast<uint4 *>(win + 8 * lane);
+          uint4 *w1 = reinterpret_cast<uint4 *>(win + kStripCols + 8 * lane);
+          w0[0] = make_uint4(vgA[0], vgA[1], vgA[2], vgA[3]);
+          w0[1] = make_uint4(vgA[4], vgA[5], vgA[6], vgA[7]);
+          w1[0] = make_uint4(vg[0], vg[1], vg[2], vg[3]);
+          w1[1] = make_uint4(vg[4], vg[5], vg[6], vg[7]);
+        } else {
+#pragma unroll
+          for (int k = 0; k < 8; k++) {
+            win[8 * lane + k] = vgA[k];
+            win[kStripCols + 8 * lane + k] = vg[k];
+          }
+        }
+        const uint32_t cntA = __popc(csA), cntB = __popc(csB);
+        uint32_t incl = cntA | (cntB << 16); // two counts of at most 256
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const uint32_t t = __shfl_up_sync(kFull, incl, d);
+          if (lane >= d)
+            incl += t;
+        }
+        const uint32_t tot = __shfl_sync(kFull, incl, 31);
+        const uint32_t totA = tot & 0xffffu, total = totA + (tot >> 16);
+        {
+          uint32_t ia = (incl & 0xffffu) - cntA, ib = totA + (incl >> 16) - cntB;
+          uint32_t left = csA;
+          while (left) {
+            cand[ia++] = static_cast<uint16_t>(8 * lane + __ffs(left) - 1);
+            left &= left - 1;
+          }
+          left = csB;
+          while (left) {
+            cand[ib++] = static_cast<uint16_t>(0x100u | (8 * lane + __ffs(left) - 1));
+            left &= left - 1;
+          }
+        }
+        __syncwarp();
+
+        // Room for both rows' candidates in one chunk, so each tile's
+        // records are contiguous whatever the rounds below find.
+        if (chunk == kNoChunk || fill + total > kChunkRecords) {
+          uint32_t base = 0;
+          if (lane == 0)
+            base = atomicAdd(args.pool_next, kChunkRecords);
+          base = __shfl_sync(kFull, base, 0);
+          if (base > args.pool_cap - kChunkRecords || base + kChunkRecords < base) {
             if (lane == 0)
-              base = atomicAdd(args.pool_next, kChunkRecords);
-            base = __shfl_sync(kFull, base, 0);
-            if (base > args.pool_cap - kChunkRecords || base + kChunkRecords < base) {
-              if (lane == 0)
-                atomicCAS(args.status, kStatusOk, kStatusPoolExhausted);
-              chunk = kNoChunk;
-            } else {
-              chunk = base;
-            }
-            fill = 0;
+              atomicCAS(args.status, kStatusOk, kStatusPoolExhausted);
+            chunk = kNoChunk;
+          } else {
+            chunk = base;
           }
-          const uint32_t start = chunk + fill;
-          const T *prow = row_at(back_slot(slot, kHalo));
-          const uint32_t row_index = static_cast<uint32_t>(c) * static_cast<uint32_t>(fd.width) +
-                                     static_cast<uint32_t>(strip * kStripOut - kHalo);
-          uint32_t found = 0;
-          for (uint32_t base = 0; base < total; base += 32) {
-            const uint32_t i = base + lane;
-            bool sig = false;
-            SignalPixel px;
-            if (i < total) {
-              const uint32_t col = cand_col[i]; // an output column: col +- 5 is in the strip
-              const uint32_t p = prow[col];
-              A h = 0;
-#pragma unroll
-              for (int d = -kRadius11; d <= kRadius11; d++)
-                h += win11[col + d];
-              if (p > 0) { // a masked pixel is never a candidate
-                sig = poisson(p, h >> Tr::kShift11, h & (C11 - 1), &px.background);
-                px.index = row_index + col;
-                px.value = p;
-                px.population = static_cast<uint16_t>(h >> Tr::kShift11);
-                px.reserved = 0;
-              }
-            }
-            const uint32_t ball = __ballot_sync(kFull, sig);
-            if (sig && chunk != kNoChunk)
-              args.pool[start + found + __popc(ball & ((1u << lane) - 1u))] = px;
-            found += __popc(ball);
-          }
-          if (found > 0) {
-            fill += found;
-            if (lane == 0) {
-              const uint64_t tile = fd.tile_base + static_cast<uint64_t>(c) * fd.strips + strip;
-              args.tile_count[tile] = found; // counted even if the records were dropped
-              args.tile_start[tile] = chunk == kNoChunk ? 0u : start;
-            }
-          }
-          __syncwarp();
+          fill = 0;
         }
+        const uint32_t start = chunk + fill;
+        const int c = rs + rr - kHalo; // frame row of row c
+        const uint32_t index0 = static_cast<uint32_t>(c) * static_cast<uint32_t>(fd.width) +
+                                static_cast<uint32_t>(strip * kStripOut - kHalo);
+        uint32_t foundA = 0, foundB = 0;
+        for (uint32_t base = 0; base < total; base += 32) {
+          const uint32_t i = base + lane;
+          bool sig = false;
+          SignalPixel px;
+          if (i < total) {
+            const uint32_t e = cand[i];
+            const uint32_t rowB = e >> 8, col = e & 0xffu; // an output column
+            const T *prow = row_at(back_slot(slot, rowB ? 9 : 10));
+            const A *w = win + (rowB ? kStripCols : 0);
+            const uint32_t pv = prow[col];
+            A h = 0;
+#pragma unroll
+            for (int d = -kRadius11; d <= kRadius11; d++)
+              h += w[col + d];
+            if (pv > 0) { // a masked pixel is never a candidate
+              sig = poisson(pv, h >> Tr::kShift11, h & (C11 - 1), &px.background);
+              px.index = index0 + (rowB ? static_cast<uint32_t>(fd.width) : 0u) + col;
+              px.value = pv;
+              px.population = static_cast<uint16_t>(h >> Tr::kShift11);
+              px.reserved = 0;
+            }
+          }
+          const uint32_t ball = __ballot_sync(kFull, sig);
+          if (sig && chunk != kNoChunk)
+            args.pool[start + foundA + foundB + __popc(ball & ((1u << lane) - 1u))] = px;
+          // the lanes holding row c's candidates: i < totA
+          const uint32_t na = totA > base ? totA - base : 0u;
+          const uint32_t rowA_lanes = na >= 32 ? kFull : (1u << na) - 1u;
+          foundA += __popc(ball & rowA_lanes);
+          foundB += __popc(ball & ~rowA_lanes);
+        }
+        if (lane == 0) {
+          const uint64_t tile = fd.tile_base + static_cast<uint64_t>(c) * fd.strips + strip;
+          // counted even if the records were dropped
+          if (foundA > 0) {
+            args.tile_count[tile] = foundA;
+            args.tile_start[tile] = chunk == kNoChunk ? 0u : start;
+          }
+          if (foundB > 0) {
+            args.tile_count[tile + fd.strips] = foundB;
+            args.tile_start[tile + fd.strips] = chunk == kNoChunk ? 0u : start + foundA;
+          }
+        }
+        fill += foundA + foundB;
+        __syncwarp();
       }
     };
 
@@ -649,14 +776,14 @@ __global__ void __launch_bounds__(WPC * 32, (sizeof(T) == 2 ? 16 : 8) / WPC)
         break;
       }
 
-      // One copy of the row body: a second (say, a warm-up-free steady
-      // state) doubles the code and the instruction cache then misses.
+      // Rows in pairs; an odd last row is paired with the arena row after it
+      // (its box holds it), whose results go nowhere.
       const int rr0 = b * kBoxRows;
       const int slot0 = st * kBoxRows;
-      const int rend = min(kBoxRows, nrows - rr0);
+      const int rend = min(kBoxRows, nrows2 - rr0);
 #pragma unroll 1
-      for (int i = 0; i < rend; i++)
-        process_row(rr0 + i, slot0 + i, std::false_type{});
+      for (int i = 0; i < rend; i += 2)
+        process_pair(rr0 + i, slot0 + i);
       __syncwarp();
     }
     if (failed) {
@@ -676,10 +803,7 @@ __global__ void __launch_bounds__(WPC * 32, (sizeof(T) == 2 ? 16 : 8) / WPC)
 
 template <typename T>
 size_t threshold_smem_bytes(int wpc) {
-  using A = typename Traits<T>::Acc;
-  return static_cast<size_t>(wpc) *
-         (kStripCols * sizeof(T) * kRingRows + kStripCols * sizeof(A) +
-          kRingStages * sizeof(uint64_t) + kStripCols);
+  return static_cast<size_t>(wpc) * WarpSmem<T>::kTotal;
 }
 
 template <typename T, int WPC>

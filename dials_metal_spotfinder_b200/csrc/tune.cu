@@ -183,7 +183,7 @@ TuneResult tune_search(int elem_bytes, int height, int width, const void *const 
     F1--;
   const std::vector<ThresholdPlan::Shape> shapes1(F1, ThresholdPlan::Shape{height, width});
   double best1 = 1e300;
-  int best_wpc = 4;
+  int best_wpc = 2;
   double best_ratio = 1.0;
   for (int wpc : {1, 2, 4}) {
     if ((elem_bytes == 2 ? threshold_occupancy<uint16_t>(wpc)

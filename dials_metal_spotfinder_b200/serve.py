@@ -130,9 +130,33 @@ def percentiles(v):
             "max": float(v.max())}
 
 
+class _NoGc:
+    """Python's cyclic garbage collector off for the replay: a full
+    collection in a process holding many arrays holds the interpreter lock
+    for tens of milliseconds, which would stall the producer threads (the
+    stand-ins for the detector) rather than anything being measured."""
+
+    def __enter__(self):
+        import gc
+        self._was = gc.isenabled()
+        gc.collect()
+        gc.disable()
+        return self
+
+    def __exit__(self, *exc):
+        import gc
+        if self._was:
+            gc.enable()
+
+
 def drive(streams, hbm_budget=0, slots=3, use_graph=True):
     """Replays every stream on its own thread at its frame rate through one
     Server and returns per-stream results (latencies in ms)."""
+    with _NoGc():
+        return _drive(streams, hbm_budget, slots, use_graph)
+
+
+def _drive(streams, hbm_budget, slots, use_graph):
     out = []
     with Server(hbm_budget=hbm_budget, slots=slots, use_graph=use_graph) as srv:
         ids = [srv.open(s.shape, two_d=s.two_d) for s in streams]
@@ -188,6 +212,12 @@ def drive_plain(streams, workers: int | None = None, give_up_s: float = 5.0):
     up). Latencies in ms from due times: frame-to-mask when the frame's list
     is on the host, frame-to-spot when the labeller has emitted the spot,
     from its last frame's due time."""
+    with _NoGc():
+        return _drive_plain(streams, workers, give_up_s)
+
+
+def _drive_plain(streams, workers, give_up_s):
+    
     import os
     import queue
 

@@ -76,7 +76,7 @@ def test_no_entry_means_the_cost_model(gpu_lib, tmp_path, monkeypatch):
     monkeypatch.setenv("SPOTFINDER_TUNE_CACHE", str(tmp_path / "empty.txt"))
     with Engine([(300, 400)] * 2, np.uint16) as eng:
         t = eng.tuning()
-    assert not t["from_cache"] and t["warps_per_block"] == 4 and t["frames_per_launch"] == 2
+    assert not t["from_cache"] and t["warps_per_block"] == 2 and t["frames_per_launch"] == 2
 
 
 def test_bad_arguments(gpu_lib):
