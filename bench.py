@@ -511,9 +511,9 @@ def run_ours(args, ranks):
 
     # threshold; placement reduce, scan, copy; grouping: setup, gather, link,
     # keep_table, flatten, mark, compact, count, rank, scatter, accept (small
-    # and large components), write, open, carry, finalize, and 5 scans of 3
+    # and large components), write, carry, finalize, and 5 scans of 3
     # launches
-    launches_per_step = 1 + 3 + (16 + 5 * 3)
+    launches_per_step = 1 + 3 + (15 + 5 * 3)
     # the whole pipeline's algorithmic bytes per frame: one read of the
     # frame, the signal list written and read back by the grouping, the
     # spot rows written

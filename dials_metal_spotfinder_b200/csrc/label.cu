@@ -26,13 +26,14 @@
 //             position
 //   rank      each finished component's emission rank; size filters
 //   scan      member offsets of the components that pass the size filters
-//   scatter   members, in any order
+//   scatter   members, in any order; each pixel's open flag (its component
+//             is not finished)
 //   accept    per component: members sorted by position (so (frame, index)
 //             order), then the FP64 pass in that order, peak-centroid
 //             filter
 //   scan      output rows and pixel offsets of the accepted spots
 //   write     spots and their pixels
-//   open/scan/carry  the open components' pixels compacted, in order, into
+//   scan/carry  the open components' pixels compacted, in order, into
 //             the other live buffer and re-rooted at their first pixel
 //   finalize  running counts and the carry for the next batch
 //
@@ -49,6 +50,10 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr uint32_t kNone = 0xffffffffu;
 constexpr int kThreads = 256;
+// Components up to this many members take lab_accept's launch with small
+// per-warp buffers (many warps per SM); the few larger ones are listed by
+// lab_rank and taken by a second launch with large buffers.
+constexpr uint32_t kSmallCap = 512;
 
 struct LabArgs {
   int32_t width;
@@ -80,6 +85,7 @@ struct LabArgs {
   Pixel *pix_tmp;
   uint64_t *pack;
   uint32_t *open;
+  uint32_t *big; // ranks of the kept components with more than kSmallCap members
   Spot *spots;
   Pixel *kept;
   uint64_t *seg_start, *seg_count;
@@ -95,6 +101,16 @@ __device__ __forceinline__ uint64_t gtid() {
 }
 __device__ __forceinline__ uint64_t gstride() {
   return static_cast<uint64_t>(gridDim.x) * blockDim.x;
+}
+
+// The root of x when no link can happen any more: read only.
+__device__ __forceinline__ uint32_t uf_root(const uint32_t *parent, uint32_t x) {
+  while (true) {
+    const uint32_t px = parent[x];
+    if (px == x)
+      return x;
+    x = px;
+  }
 }
 
 // Union-find on positions. Parents only ever point to lower positions.
@@ -211,6 +227,7 @@ __global__ void lab_setup(LabArgs a) {
   sc->signal_pixels += pos - carry;
   sc->closed32 = sc->open32 = 0;
   sc->runs_n = 0;
+  sc->big_n = 0;
   sc->members_pack = 0;
   sc->accepted_pack = 0;
 }
@@ -318,10 +335,10 @@ __global__ void __launch_bounds__(kThreads) lab_gather(LabArgs a) {
 }
 
 // First position (relative to the list at s0) whose index is at least t,
-// or count.
-__device__ __forceinline__ uint64_t first_at_least(const LabArgs &a, const uint32_t *tab,
-                                                   uint64_t s0, uint64_t count, uint32_t t) {
-  const uint32_t p = tab[t >> kBlockShift];
+// or count, given the block table's entry p for t (loaded by the caller, so
+// that independent lookups overlap).
+__device__ __forceinline__ uint64_t first_at_least(const LabArgs &a, uint32_t p, uint64_t s0,
+                                                   uint64_t count, uint32_t t) {
   uint64_t q = p == kNone ? count : p;
   while (q < count && a.ix[s0 + q] < t)
     q++;
@@ -330,13 +347,11 @@ __device__ __forceinline__ uint64_t first_at_least(const LabArgs &a, const uint3
 
 // Unites the tree of `ra` (the run whose first pixel is g, or an ancestor)
 // with every run of the list at s0 that has a pixel with an index in
-// [lo, hi] (one row's span, at most 32 indices): the run holding the first
-// such pixel, then the later run starts, found in the run-start bitmap;
-// returns the merged root.
-__device__ __forceinline__ uint32_t unite_overlaps(const LabArgs &a, uint32_t ra,
-                                                   const uint32_t *tab, uint64_t s0,
-                                                   uint64_t count, uint32_t lo, uint32_t hi) {
-  const uint64_t q = first_at_least(a, tab, s0, count, lo);
+// [lo, hi] (one row's span, at most 32 indices), q being the first position
+// at or past lo: the run holding that pixel, then the later run starts,
+// found in the run-start bitmap; returns the merged root.
+__device__ __forceinline__ uint32_t unite_overlaps(const LabArgs &a, uint32_t ra, uint64_t q,
+                                                   uint64_t s0, uint64_t count, uint32_t hi) {
   if (q >= count)
     return ra;
   uint64_t p = s0 + q;
@@ -392,12 +407,22 @@ __global__ void __launch_bounds__(kThreads) lab_link(LabArgs a) {
     const uint64_t end = s0 + a.seg_count[s];
     const uint32_t idx = a.ix[g];
     const uint32_t last = idx + len - 1; // the piece's last index (one row, one chunk)
-    if (idx >= W)
-      ra = unite_overlaps(a, ra, table_of(a, s, first_batch_seg), s0, end - s0, idx - W,
-                          last - W);
-    if (!a.two_d && s > 0 && a.seg_z[s - 1] + 1 == a.seg_z[s])
-      unite_overlaps(a, ra, table_of(a, s - 1, first_batch_seg), a.seg_start[s - 1],
-                     a.seg_count[s - 1], idx, last);
+    const bool up = idx >= W;
+    const bool prev = !a.two_d && s > 0 && a.seg_z[s - 1] + 1 == a.seg_z[s];
+    // both lookups' first loads before either walk
+    const uint32_t tu = up ? table_of(a, s, first_batch_seg)[(idx - W) >> kBlockShift] : kNone;
+    const uint32_t tp = prev ? table_of(a, s - 1, first_batch_seg)[idx >> kBlockShift] : kNone;
+    const uint64_t qu = up ? first_at_least(a, tu, s0, end - s0, idx - W) : end - s0;
+    uint64_t ps0 = 0, pcount = 0, qp = 0;
+    if (prev) {
+      ps0 = a.seg_start[s - 1];
+      pcount = a.seg_count[s - 1];
+      qp = first_at_least(a, tp, ps0, pcount, idx);
+    }
+    if (up)
+      ra = unite_overlaps(a, ra, qu, s0, end - s0, last - W);
+    if (prev)
+      unite_overlaps(a, ra, qp, ps0, pcount, last);
   }
 }
 
@@ -422,7 +447,7 @@ __global__ void __launch_bounds__(kThreads) lab_flatten(LabArgs a) {
     uint32_t r = kNone;
     int32_t z = INT_MIN;
     if (g < n) {
-      r = uf_find(a.par, static_cast<uint32_t>(g));
+      r = uf_root(a.par, static_cast<uint32_t>(g)); // lab_link is done: no more links
       a.root[g] = r;
       z = a.fr[g];
     }
@@ -515,6 +540,8 @@ __global__ void __launch_bounds__(kThreads) lab_rank(LabArgs a) {
     const bool keep = size >= a.min_size && size <= a.max_size;
     a.msize[rank] = keep ? size : 0u;
     a.mpk[rank] = keep ? (static_cast<uint64_t>(size) | (1ull << 32)) : 0ull;
+    if (keep && size > kSmallCap)
+      a.big[atomicAdd(&sc->big_n, 1u)] = rank;
     small += size < a.min_size;
     large += size > a.max_size;
   }
@@ -524,8 +551,10 @@ __global__ void __launch_bounds__(kThreads) lab_rank(LabArgs a) {
     atomicAdd(reinterpret_cast<unsigned long long *>(&sc->too_large), large);
 }
 
-// Member lists. A warp takes 32 consecutive positions; the lanes of one
-// component claim their slots with one atomic and fill them in lane order.
+// Member lists, and the open flags of every pixel (its component is not
+// finished by this batch, so it is carried). A warp takes 32 consecutive
+// positions; the lanes of one component claim their slots with one atomic
+// and fill them in lane order.
 // So each component's list is a set of runs, one per 32-position chunk it
 // has pixels in, each run ascending and within its chunk; lab_accept orders
 // the runs rather than the members.
@@ -539,6 +568,8 @@ __global__ void __launch_bounds__(kThreads) lab_scatter(LabArgs a) {
     if (g < n) {
       r = a.root[g];
       rank = a.rank_of_root[r];
+      // a pixel of a component not finished by this batch is carried
+      a.open[g] = rank == kNone ? 1u : 0u;
       if (rank != kNone && a.msize[rank] == 0)
         rank = kNone;
     }
@@ -707,7 +738,6 @@ struct WarpBuffers {
 // Per warp: four CAP-member arrays and the terms. Two launches split the
 // components by size: up to kSmallCap members with small buffers, so that
 // many warps fit on an SM, and the rest with kCompCap-member buffers.
-constexpr uint32_t kSmallCap = 512;
 
 template <uint32_t CAP> __host__ __device__ constexpr size_t warp_comp_bytes() {
   return 4 * CAP * sizeof(uint32_t) + 3 * 32 * sizeof(double);
@@ -1017,18 +1047,21 @@ __device__ bool spot_pass_warp(uint32_t W, double max_sep, const WarpBuffers &b,
 // where the accepted ones go.
 // Components of lo < size <= hi; the launch with lo = 0 also clears the
 // pack word of those the size filter removed.
+// With `listed`, the components are lab_rank's list of the large ones
+// rather than every finished root.
 template <uint32_t CAP>
 __global__ void __launch_bounds__(kCompWarps * 32) lab_accept(LabArgs a, uint32_t lo,
-                                                              uint32_t hi) {
+                                                              uint32_t hi, int listed) {
   extern __shared__ __align__(16) unsigned char comp_smem[];
   LabelScalars *sc = a.sc;
-  const uint64_t closed = sc->closed;
+  const uint64_t closed = listed ? sc->big_n : sc->closed;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const WarpBuffers b = warp_buffers<CAP>(comp_smem, warp);
   const uint32_t W = static_cast<uint32_t>(a.width);
   uint32_t separated = 0;
   const uint64_t gw = gtid() >> 5, nw = gstride() >> 5;
-  for (uint64_t r = gw; r < closed; r += nw) {
+  for (uint64_t i = gw; i < closed; i += nw) {
+    const uint64_t r = listed ? a.big[i] : i;
     const uint32_t n = a.msize[r];
     if (n == 0) {
       if (lane == 0 && lo == 0)
@@ -1118,20 +1151,19 @@ __global__ void __launch_bounds__(kThreads) lab_write(LabArgs a) {
 }
 
 
-__global__ void __launch_bounds__(kThreads) lab_open(LabArgs a) {
-  const uint64_t n = a.sc->n;
-  for (uint64_t g = gtid(); g < n; g += gstride())
-    a.open[g] = a.rank_of_root[a.root[g]] == kNone ? 1u : 0u;
-}
-
+// The open pixels to the other live buffer, in order. `open` holds the
+// exclusive scan of lab_scatter's open flags, so a pixel is open where the
+// scan steps up after it (the total after the last pixel).
 __global__ void __launch_bounds__(kThreads) lab_carry(LabArgs a) {
   LabelScalars *sc = a.sc;
   const uint64_t n = sc->n;
+  const uint32_t total = sc->open32;
   for (uint64_t g = gtid(); g < n; g += gstride()) {
-    const uint32_t r = a.root[g];
-    if (a.rank_of_root[r] != kNone)
+    const uint32_t at = a.open[g];
+    const uint32_t next = g + 1 < n ? a.open[g + 1] : total;
+    if (next == at)
       continue;
-    const uint32_t at = a.open[g]; // exclusive scan of the open flags
+    const uint32_t r = a.root[g];
     a.nfr[at] = a.fr[g];
     a.nix[at] = a.ix[g];
     a.nval[at] = a.val[g];
@@ -1215,13 +1247,13 @@ void DeviceLabeller::release() {
   }
   void *ptrs[] = {root_, size_, rank_of_root_, cursor_, lastz_, bits_, bcnt_, flist_, comp_root_,
                   msize_, mpk_, runs_, run_starts_, spot_tmp_, pix_tmp_, members_, pack_, open_, spots_out_, kept_out_, seg_start_,
-                  seg_count_, seg_z_, tab_};
+                  seg_count_, seg_z_, tab_, big_};
   for (void *p : ptrs)
     cudaFree(p);
   tab_ = nullptr;
   root_ = size_ = rank_of_root_ = cursor_ = nullptr;
   lastz_ = nullptr;
-  bits_ = bcnt_ = flist_ = comp_root_ = msize_ = members_ = open_ = nullptr;
+  bits_ = bcnt_ = flist_ = comp_root_ = msize_ = members_ = open_ = big_ = nullptr;
   mpk_ = pack_ = nullptr;
   runs_ = nullptr;
   run_starts_ = nullptr;
@@ -1285,6 +1317,7 @@ void DeviceLabeller::reserve(uint64_t batch_pixels, int max_frames, uint64_t car
     alloc(&members_, live, "members");
     alloc(&pack_, live, "spot offsets");
     alloc(&open_, live, "open flags");
+    alloc(&big_, live / (kSmallCap + 1) + 1, "large components");
     alloc(&spots_out_, spot_cap, "spots");
     alloc(&spot_tmp_, spot_cap, "spot scratch");
     alloc(&pix_tmp_, live, "spot pixel scratch");
@@ -1374,6 +1407,7 @@ void DeviceLabeller::enqueue(int nframes, const SignalPixel *lists, const uint64
   a.members = members_;
   a.pack = pack_;
   a.open = open_;
+  a.big = big_;
   a.spots = spots_out_;
   a.kept = kept_out_;
   a.seg_start = seg_start_;
@@ -1408,14 +1442,13 @@ void DeviceLabeller::enqueue(int nframes, const SignalPixel *lists, const uint64
   check(cudaEventRecord(fork_, s), "cudaEventRecord");
   check(cudaStreamWaitEvent(aux_, fork_, 0), "cudaStreamWaitEvent");
   lab_accept<kCompCap><<<grid_ / 4, kCompWarps * 32, kCompWarps * warp_comp_bytes<kCompCap>(),
-                         aux_>>>(a, kSmallCap, 0xffffffffu);
+                         aux_>>>(a, kSmallCap, 0xffffffffu, 1);
   lab_accept<kSmallCap><<<grid, kCompWarps * 32, kCompWarps * warp_comp_bytes<kSmallCap>(), s>>>(
-      a, 0u, kSmallCap);
+      a, 0u, kSmallCap, 0);
   check(cudaEventRecord(join_, aux_), "cudaEventRecord");
   check(cudaStreamWaitEvent(s, join_, 0), "cudaStreamWaitEvent");
   scan64_.run(pack_, pack_, &sc->closed, 1, live_cap_, &sc->accepted_pack, s);
   lab_write<<<grid, kThreads, 0, s>>>(a);
-  lab_open<<<grid, kThreads, 0, s>>>(a);
   scan32_.run(open_, open_, &sc->n, 1, live_cap_, &sc->open32, s);
   lab_carry<<<grid, kThreads, 0, s>>>(a);
   lab_finalize<<<1, 32, 0, s>>>(a);
