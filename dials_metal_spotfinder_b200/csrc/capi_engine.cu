@@ -77,7 +77,7 @@ int sf_engine_create(int elem_bytes, int nframes, const int32_t *heights,
     bool automatic = true;
     if (config) {
       t.seg_rows = config->seg_rows;
-      t.warps_per_block = config->warps_per_block > 0 ? config->warps_per_block : 2;
+      t.warps_per_block = config->warps_per_block > 0 ? config->warps_per_block : 0;
       t.blocks_per_sm = config->blocks_per_sm;
       slots = config->slots > 0 ? config->slots : 1;
       automatic = config->seg_rows == 0 && config->warps_per_block == 0;

@@ -104,6 +104,10 @@ ThresholdPlan::ThresholdPlan(int elem_bytes, const std::vector<Shape> &shapes,
     throw std::invalid_argument("a plan needs at least one frame");
   if (slots < 1)
     throw std::invalid_argument("a plan needs at least one slot");
+  // 16-bit pixels: 7 two-warp blocks per SM; 32-bit: each warp's shared
+  // memory is twice the size, so one-warp blocks fill the SM best
+  if (tuning_.warps_per_block == 0)
+    tuning_.warps_per_block = elem_bytes == 2 ? 2 : 1;
   const int wpc = tuning_.warps_per_block;
   if (wpc != 1 && wpc != 2 && wpc != 4)
     throw std::invalid_argument("warps_per_block must be 1, 2 or 4");

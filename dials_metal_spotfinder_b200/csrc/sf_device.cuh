@@ -32,8 +32,8 @@ constexpr int kHalo = 10;                  // 3 (7x7) + 2 (5x5) + 5 (11x11)
 constexpr int kStripOut = 232;             // outputs per strip
 constexpr int kMarginLeft = kHalo;         // frame column 0 at buffer column 10
 constexpr int kMarginRows = kHalo;         // rows of fill above and below
-constexpr int kRingRows = 24;              // rows of a strip held in smem
-constexpr int kBoxRows = 4;                // rows per TMA box
+constexpr int kRingRows = 20;              // rows of a strip held in smem
+constexpr int kBoxRows = 2;                // rows per TMA box
 constexpr int kRingStages = kRingRows / kBoxRows;
 constexpr uint32_t kChunkRecords = 1024;   // staging pool allocation unit
 // The most records a warp stages at once (two output rows of a strip); a

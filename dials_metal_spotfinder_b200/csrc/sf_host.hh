@@ -84,7 +84,7 @@ int device_sm_count();
 // Launch geometry of the threshold for one batch shape.
 struct PlanTuning {
   int seg_rows = 0;        // output rows per task; 0 picks by frame count
-  int warps_per_block = 2; // 1, 2 or 4
+  int warps_per_block = 0; // 1, 2 or 4; 0: 2 for 16-bit pixels, 1 for 32-bit
   int blocks_per_sm = 0;   // 0: as many as fit
 };
 

@@ -337,13 +337,18 @@ __device__ __forceinline__ int back_slot(int slot, int back) {
 }
 
 // Warps per SM the shared memory holds: a warp's ring, the 11-row sums of
-// two rows and their candidate list (15 KB for 16-bit pixels, 30 KB for
+// two rows and their candidate list (13 KB for 16-bit pixels, 25 KB for
 // 32-bit).
-template <typename T> constexpr int kWarpsPerSm = sizeof(T) == 2 ? 14 : 7;
+template <typename T> constexpr int kWarpsPerSm = sizeof(T) == 2 ? 16 : 8;
 
 // The rows before a task's first are read as zeros: 16 rows, the farthest
 // back any row's sums reach (the 11-row window's leaving row, 16 above).
 constexpr int kPreRows = 16;
+// A pair of rows r, r+1 reads rows r-16 .. r+1 while the next box is in
+// flight; the first two boxes do not land on the zero rows.
+static_assert(kRingRows >= kPreRows + 2 + kBoxRows, "ring too short");
+static_assert(kRingRows - kPreRows >= 2 * kBoxRows, "prologue boxes overlap the zero rows");
+static_assert(kBoxRows % 2 == 0 && kRingRows % kBoxRows == 0, "rows go in pairs");
 
 // Per-warp shared memory (the square-root table is static).
 template <typename T> struct WarpSmem {
@@ -759,8 +764,8 @@ __global__ void __launch_bounds__(WPC * 32, (kWarpsPerSm<T> / WPC) > 0 ? kWarpsP
     for (int b = 0; b < nboxes && !failed; b++) {
       const int st = b % kRingStages;
       if (lane == 0 && b >= 1 && b + 1 < nboxes) {
-        // Box b+1 reuses the stage of box b-5, whose rows are all older than
-        // r-16 for every row of box b: free.
+        // Box b+1 reuses the stage of box b+1-kRingStages, whose rows are
+        // all older than r-16 for every row of box b: free.
         const int nst = (b + 1) % kRingStages;
         fence_proxy_async_smem();
         mbar_expect_tx(&bars[nst], kBoxBytes);

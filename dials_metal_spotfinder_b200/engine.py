@@ -16,7 +16,7 @@ from ._lib import (COUNT_NAMES, PIXEL, SIGNAL_PIXEL, SPOT, EngineConfig, GroupOp
 class Engine:
     """seg_rows and warps_per_block 0 (the default): the tuner file's choice
     for this frame shape on this device (see tune.py), else the cost model's
-    task height and 2 warps per block."""
+    task height and 2 warps per block (1 for 32-bit pixels)."""
 
     def __init__(self, shapes, dtype=np.uint16, slots=1, seg_rows=0, warps_per_block=0,
                  blocks_per_sm=0):

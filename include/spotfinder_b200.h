@@ -235,14 +235,15 @@ typedef struct sf_engine sf_engine;
 
 typedef struct sf_engine_config {
   int32_t seg_rows;        /* output rows per warp task; 0 = tuned or the cost model's */
-  int32_t warps_per_block; /* 1, 2 or 4; 0 = tuned, else 2 */
+  int32_t warps_per_block; /* 1, 2 or 4; 0 = tuned, else 2 (16-bit) or 1 (32-bit) */
   int32_t blocks_per_sm;   /* 0 = as many as fit */
   int32_t slots;           /* device arenas; 0 = 1 */
 } sf_engine_config;
 /* With seg_rows and warps_per_block both 0 (or no config), an engine whose
  * frames all have one shape reads the tuner file (sf_tune) for that shape on
  * this kind of device and uses its warps per block and task height; without
- * an entry it uses the cost model and 2 warps per block. */
+ * an entry it uses the cost model and 2 warps per block (1 for 32-bit
+ * pixels). */
 
 SF_API int sf_engine_create(int elem_bytes, int nframes, const int32_t *heights,
                             const int32_t *widths, const sf_engine_config *config,
