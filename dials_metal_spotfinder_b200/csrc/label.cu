@@ -54,10 +54,6 @@ constexpr int kThreads = 256;
 // per-warp buffers (many warps per SM); the few larger ones are listed by
 // lab_rank and taken by a second launch with large buffers.
 constexpr uint32_t kSmallCap = 512;
-// Components up to this many members, in at most kLaneRuns chunk runs, are
-// taken one per thread by lab_accept_lanes; the rest by a warp each.
-constexpr uint32_t kLaneCap = 128;
-constexpr uint32_t kLaneRuns = 32;
 
 struct LabArgs {
   int32_t width;
@@ -90,7 +86,6 @@ struct LabArgs {
   uint64_t *pack;
   uint32_t *open;
   uint32_t *big; // ranks of the kept components with more than kSmallCap members
-  uint32_t *mid; // ranks of those the per-lane pass leaves to the warp pass
   Spot *spots;
   Pixel *kept;
   uint64_t *seg_start, *seg_count;
@@ -233,7 +228,7 @@ __global__ void lab_setup(LabArgs a) {
   sc->closed32 = sc->open32 = 0;
   sc->runs_n = 0;
   sc->big_n = 0;
-  sc->mid_n = 0;
+  sc->link_next = sc->accept_next = sc->big_next = 0;
   sc->members_pack = 0;
   sc->accepted_pack = 0;
 }
@@ -392,15 +387,26 @@ __device__ __forceinline__ uint32_t unite_overlaps(const LabArgs &a, uint32_t ra
 // above, and of the previous frame's same row, that overlaps its span: each
 // up or previous-frame edge of the run's pixels ends in one of those runs.
 __global__ void __launch_bounds__(kThreads) lab_link(LabArgs a) {
-  const LabelScalars *sc = a.sc;
+  LabelScalars *sc = a.sc;
   const uint64_t carry = sc->carry_n;
   const int first_batch_seg = carry > 0 ? 1 : 0;
   const uint32_t W = static_cast<uint32_t>(a.width);
   const int64_t z0 = sc->batch_z0;
   const uint32_t nruns = sc->runs_n;
-  // one entry of lab_gather's list per thread, so the lanes of a warp all
-  // have a run to link
-  for (uint64_t i = gtid(); i < nruns; i += gstride()) {
+  const int lane = threadIdx.x & 31;
+  // one entry of lab_gather's list per lane, so the lanes of a warp all
+  // have a run to link; a warp takes the next 32 entries when its last are
+  // done (chains vary in length, so fixed shares would leave warps idle)
+  while (true) {
+    uint32_t base = 0;
+    if (lane == 0)
+      base = atomicAdd(&sc->link_next, 32u);
+    base = __shfl_sync(kFull, base, 0);
+    if (base >= nruns)
+      break;
+    const uint64_t i = base + static_cast<uint64_t>(lane);
+    if (i >= nruns)
+      continue;
     const uint64_t e = a.runs[i];
     const uint64_t g = e & 0xffffffffu;
     const uint32_t len = static_cast<uint32_t>(e >> 32) & 0x3fu;
@@ -548,8 +554,6 @@ __global__ void __launch_bounds__(kThreads) lab_rank(LabArgs a) {
     a.mpk[rank] = keep ? (static_cast<uint64_t>(size) | (1ull << 32)) : 0ull;
     if (keep && size > kSmallCap)
       a.big[atomicAdd(&sc->big_n, 1u)] = rank;
-    else if (keep && size > kLaneCap)
-      a.mid[atomicAdd(&sc->mid_n, 1u)] = rank;
     small += size < a.min_size;
     large += size > a.max_size;
   }
@@ -1055,21 +1059,28 @@ __device__ bool spot_pass_warp(uint32_t W, double max_sep, const WarpBuffers &b,
 // where the accepted ones go.
 // Components of lo < size <= hi; the launch with lo = 0 also clears the
 // pack word of those the size filter removed.
-// `listed` 1: the components of lab_rank's list of the large ones; 2: the
-// list of those lab_accept_lanes leaves to a warp; 0: every finished root.
+// With `listed`, the components are lab_rank's list of the large ones
+// rather than every finished root.
 template <uint32_t CAP>
 __global__ void __launch_bounds__(kCompWarps * 32) lab_accept(LabArgs a, uint32_t lo,
                                                               uint32_t hi, int listed) {
   extern __shared__ __align__(16) unsigned char comp_smem[];
   LabelScalars *sc = a.sc;
-  const uint64_t closed = listed == 1 ? sc->big_n : listed == 2 ? sc->mid_n : sc->closed;
+  const uint64_t closed = listed ? sc->big_n : sc->closed;
+  uint32_t *next = listed ? &sc->big_next : &sc->accept_next;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const WarpBuffers b = warp_buffers<CAP>(comp_smem, warp);
   const uint32_t W = static_cast<uint32_t>(a.width);
   uint32_t separated = 0;
-  const uint64_t gw = gtid() >> 5, nw = gstride() >> 5;
-  for (uint64_t i = gw; i < closed; i += nw) {
-    const uint64_t r = listed == 1 ? a.big[i] : listed == 2 ? a.mid[i] : i;
+  // a warp takes the next component when it has finished its last
+  while (true) {
+    uint32_t i = 0;
+    if (lane == 0)
+      i = atomicAdd(next, 1u);
+    i = __shfl_sync(kFull, i, 0);
+    if (i >= closed)
+      break;
+    const uint64_t r = listed ? a.big[i] : i;
     const uint32_t n = a.msize[r];
     if (n == 0) {
       if (lane == 0 && lo == 0)
@@ -1125,132 +1136,6 @@ __global__ void __launch_bounds__(kCompWarps * 32) lab_accept(LabArgs a, uint32_
     __syncwarp();
   }
   if (lane == 0 && separated)
-    atomicAdd(reinterpret_cast<unsigned long long *>(&sc->separated), separated);
-}
-
-// A component's members in position order, one at a time, for a pass run by
-// one thread: its member list is one ascending run per 32-position chunk
-// (lab_scatter), and the runs' heads, sorted by chunk, are in shared memory
-// (run j's chunk at key[32 j], its start | length << 16 at head[32 j],
-// interleaved with the warp's other lanes). get() is called for k = 0, 1,
-// ..., n-1 in turn, and again from 0 for the second pass.
-struct LaneRunMembers {
-  const LabArgs *a;
-  const uint32_t *m;
-  const uint32_t *head; // this lane's column
-  mutable uint32_t j, off, start, len;
-  __device__ __forceinline__ void get(uint32_t k, uint32_t *idx, uint32_t *v, int32_t *z) const {
-    if (k == 0) {
-      j = 0;
-      off = 0;
-    } else if (++off == len) {
-      j++;
-      off = 0;
-    }
-    if (off == 0) {
-      const uint32_t h = head[32 * j];
-      start = h & 0xffffu;
-      len = h >> 16;
-    }
-    const uint32_t g = m[start + off];
-    *idx = a->ix[g];
-    *v = a->val[g];
-    *z = a->fr[g];
-  }
-};
-
-// The spot pass for the many small components, one per thread: the same
-// sequential arithmetic as the reference (spot_pass, member order), with 32
-// components in flight per warp instead of one, which is what keeps the
-// device busy when the passes are latency-bound. Components that pass the
-// size filters with more than kLaneCap members are already on lab_rank's
-// lists; one whose members lie in more than kLaneRuns chunks is put on the
-// list of the warp pass with small buffers. Also clears the pack word of
-// the components the size filter removed.
-constexpr int kLaneWarps = 4;
-
-__global__ void __launch_bounds__(kLaneWarps * 32) lab_accept_lanes(LabArgs a) {
-  __shared__ uint32_t keys[kLaneWarps][kLaneRuns * 32];
-  __shared__ uint32_t heads[kLaneWarps][kLaneRuns * 32];
-  LabelScalars *sc = a.sc;
-  const uint64_t closed = sc->closed;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint32_t *key = &keys[warp][lane];
-  uint32_t *head = &heads[warp][lane];
-  const uint32_t W = static_cast<uint32_t>(a.width);
-  uint32_t separated = 0;
-  for (uint64_t r = gtid(); r < closed; r += gstride()) {
-    const uint32_t n = a.msize[r];
-    if (n == 0) {
-      a.pack[r] = 0;
-      continue;
-    }
-    if (n > kLaneCap)
-      continue;
-    const uint32_t moff = static_cast<uint32_t>(a.mpk[r]);
-    const uint32_t sidx = static_cast<uint32_t>(a.mpk[r] >> 32);
-    const uint32_t *m = a.members + moff;
-    // the runs, in list order
-    uint32_t nr = 0, prev = kNone, run0 = 0;
-    bool many = false;
-    for (uint32_t k = 0; k < n; k++) {
-      const uint32_t c = m[k] >> 5;
-      if (c != prev) {
-        if (nr > 0)
-          head[32 * (nr - 1)] = run0 | ((k - run0) << 16);
-        if (nr == kLaneRuns) {
-          many = true;
-          break;
-        }
-        key[32 * nr] = c;
-        run0 = k;
-        prev = c;
-        nr++;
-      }
-    }
-    if (many) {
-      a.mid[atomicAdd(&sc->mid_n, 1u)] = static_cast<uint32_t>(r);
-      continue;
-    }
-    head[32 * (nr - 1)] = run0 | ((n - run0) << 16);
-    // the runs by chunk (chunks are distinct): insertion sort
-    for (uint32_t i = 1; i < nr; i++) {
-      const uint32_t kc = key[32 * i], hc = head[32 * i];
-      uint32_t j = i;
-      while (j > 0 && key[32 * (j - 1)] > kc) {
-        key[32 * j] = key[32 * (j - 1)];
-        head[32 * j] = head[32 * (j - 1)];
-        j--;
-      }
-      key[32 * j] = kc;
-      head[32 * j] = hc;
-    }
-    Spot spot{}; // zeroed, padding included, so rows compare byte for byte
-    const LaneRunMembers mem{&a, m, head, 0, 0, 0, 0};
-    const bool ok = spot_pass(W, a.max_sep, mem, n, &spot);
-    for (uint32_t k = 0; k < n; k++) {
-      Pixel p;
-      uint32_t idx, v;
-      int32_t z;
-      mem.get(k, &idx, &v, &z);
-      p.frame = z;
-      p.index = idx;
-      p.value = v;
-      a.pix_tmp[moff + k] = p;
-    }
-    if (sidx < a.spot_cap)
-      a.spot_tmp[sidx] = spot;
-    else
-      sc->status = kLabelSpotOverflow;
-    if (!ok) {
-      separated++;
-      a.msize[r] = 0;
-      a.pack[r] = 0;
-    } else {
-      a.pack[r] = (static_cast<uint64_t>(n) << 32) | 1u;
-    }
-  }
-  if (separated)
     atomicAdd(reinterpret_cast<unsigned long long *>(&sc->separated), separated);
 }
 
@@ -1381,13 +1266,13 @@ void DeviceLabeller::release() {
   }
   void *ptrs[] = {root_, size_, rank_of_root_, cursor_, lastz_, bits_, bcnt_, flist_, comp_root_,
                   msize_, mpk_, runs_, run_starts_, spot_tmp_, pix_tmp_, members_, pack_, open_, spots_out_, kept_out_, seg_start_,
-                  seg_count_, seg_z_, tab_, big_, mid_};
+                  seg_count_, seg_z_, tab_, big_};
   for (void *p : ptrs)
     cudaFree(p);
   tab_ = nullptr;
   root_ = size_ = rank_of_root_ = cursor_ = nullptr;
   lastz_ = nullptr;
-  bits_ = bcnt_ = flist_ = comp_root_ = msize_ = members_ = open_ = big_ = mid_ = nullptr;
+  bits_ = bcnt_ = flist_ = comp_root_ = msize_ = members_ = open_ = big_ = nullptr;
   mpk_ = pack_ = nullptr;
   runs_ = nullptr;
   run_starts_ = nullptr;
@@ -1452,9 +1337,6 @@ void DeviceLabeller::reserve(uint64_t batch_pixels, int max_frames, uint64_t car
     alloc(&pack_, live, "spot offsets");
     alloc(&open_, live, "open flags");
     alloc(&big_, live / (kSmallCap + 1) + 1, "large components");
-    // kLaneCap < size <= kSmallCap, or more than kLaneRuns runs (so more
-    // than kLaneRuns members)
-    alloc(&mid_, live / (kLaneRuns + 1) + 1, "warp-pass components");
     alloc(&spots_out_, spot_cap, "spots");
     alloc(&spot_tmp_, spot_cap, "spot scratch");
     alloc(&pix_tmp_, live, "spot pixel scratch");
@@ -1545,7 +1427,6 @@ void DeviceLabeller::enqueue(int nframes, const SignalPixel *lists, const uint64
   a.pack = pack_;
   a.open = open_;
   a.big = big_;
-  a.mid = mid_;
   a.spots = spots_out_;
   a.kept = kept_out_;
   a.seg_start = seg_start_;
@@ -1581,9 +1462,8 @@ void DeviceLabeller::enqueue(int nframes, const SignalPixel *lists, const uint64
   check(cudaStreamWaitEvent(aux_, fork_, 0), "cudaStreamWaitEvent");
   lab_accept<kCompCap><<<grid_ / 4, kCompWarps * 32, kCompWarps * warp_comp_bytes<kCompCap>(),
                          aux_>>>(a, kSmallCap, 0xffffffffu, 1);
-  lab_accept_lanes<<<grid, kLaneWarps * 32, 0, s>>>(a);
   lab_accept<kSmallCap><<<grid, kCompWarps * 32, kCompWarps * warp_comp_bytes<kSmallCap>(), s>>>(
-      a, 0u, kSmallCap, 2);
+      a, 0u, kSmallCap, 0);
   check(cudaEventRecord(join_, aux_), "cudaEventRecord");
   check(cudaStreamWaitEvent(s, join_, 0), "cudaStreamWaitEvent");
   scan64_.run(pack_, pack_, &sc->closed, 1, live_cap_, &sc->accepted_pack, s);

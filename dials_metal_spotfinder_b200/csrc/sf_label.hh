@@ -52,8 +52,10 @@ struct LabelScalars {
   uint32_t closed32, open32;
   uint32_t runs_n;        // lab_link's work list
   uint32_t big_n;         // components past the small spot-pass buffers
-  uint32_t mid_n;         // components for the warp spot pass with small buffers
-  uint32_t pad0;
+  // work counters: warps take the next entries as they finish their last,
+  // so a few long union-find chains or large components do not hold a
+  // whole grid-stride share
+  uint32_t link_next, accept_next, big_next, pad0;
   uint64_t members_pack;  // members (low 32) | components passing the size filters (high 32)
   uint64_t accepted_pack; // accepted spots (low 32) | their pixels (high 32)
   uint64_t batch_spots, batch_pixels;
@@ -142,7 +144,6 @@ private:
   uint64_t *pack_ = nullptr;
   uint32_t *open_ = nullptr;
   uint32_t *big_ = nullptr; // ranks of the components lab_accept's large launch takes
-  uint32_t *mid_ = nullptr; // ... and its launch with small buffers
   Spot *spots_out_ = nullptr;
   Pixel *kept_out_ = nullptr;
   uint64_t *seg_start_ = nullptr; // per batch segment: start, count (device)
