@@ -79,7 +79,7 @@ struct LabArgs {
   uint32_t *flist;       // the finished roots in position order
   uint32_t *comp_root, *msize, *members;
   uint64_t *mpk;
-  uint64_t *runs; // per batch: lab_link's entries, see lab_gather
+  uint4 *runs; // per batch: lab_link's entries, see lab_gather
   uint32_t *run_starts; // bit p & 31 of word p >> 5: position p starts a run
   Spot *spot_tmp;
   Pixel *pix_tmp;
@@ -264,6 +264,8 @@ __global__ void __launch_bounds__(kThreads) lab_gather(LabArgs a) {
     const uint64_t base = block_base + static_cast<uint64_t>(warp) * 32;
     const uint64_t g = base + lane;
     bool left = false;
+    int seg = 0;       // a new pixel's frame segment
+    uint32_t pidx = 0; // and its index, for the work list
     if (g < n) {
       a.size[g] = 0;
       a.lastz[g] = INT_MIN;
@@ -271,6 +273,7 @@ __global__ void __launch_bounds__(kThreads) lab_gather(LabArgs a) {
       a.cursor[g] = 0;
       if (g >= carry) {
         const int s = segment_of(a.seg_start, nseg, g);
+        seg = s;
         const int f = s - first_batch_seg;
         const uint64_t i = g - a.seg_start[s];
         const SignalPixel *list = a.lists + a.offs[f];
@@ -278,6 +281,7 @@ __global__ void __launch_bounds__(kThreads) lab_gather(LabArgs a) {
         a.fr[g] = static_cast<int32_t>(a.seg_z[s]);
         a.ix[g] = px.index;
         a.val[g] = px.value;
+        pidx = px.index;
         const uint32_t prev = i == 0 ? 0u : list[i - 1].index;
         left = i > 0 && px.index % W != 0 && prev + 1 == px.index;
         // This pixel is the first of every block from the one after the
@@ -305,8 +309,10 @@ __global__ void __launch_bounds__(kThreads) lab_gather(LabArgs a) {
       a.par[g] = static_cast<uint32_t>(base + first);
     }
     // lab_link's work list: one entry per piece of a run within a chunk --
-    // its first position, its length and whether it continues a run from
-    // the chunk before (lane 0 joined to its left neighbour)
+    // its first position, its first pixel's index, its length, whether it
+    // continues a run from the chunk before (lane 0 joined to its left
+    // neighbour) and its frame segment, so that lab_link starts from one
+    // 16-byte load
     const bool boundary = left && lane == 0;
     const bool entry = mine && (!left || boundary);
     const uint32_t want = __ballot_sync(kFull, entry);
@@ -330,7 +336,8 @@ __global__ void __launch_bounds__(kThreads) lab_gather(LabArgs a) {
     __syncthreads();
     if (entry)
       a.runs[block_at + warp_count[warp] + __popc(want & ((1u << lane) - 1u))] =
-          g | (static_cast<uint64_t>(len) << 32) | (boundary ? (1ull << 40) : 0ull);
+          make_uint4(static_cast<uint32_t>(g), pidx,
+                     len | (boundary ? 0x40u : 0u) | (static_cast<uint32_t>(seg) << 8), 0u);
     __syncthreads();
   }
 }
@@ -386,13 +393,31 @@ __device__ __forceinline__ uint32_t unite_overlaps(const LabArgs &a, uint32_t ra
 // here. The first pixel of each run then unites it with every run of the row
 // above, and of the previous frame's same row, that overlaps its span: each
 // up or previous-frame edge of the run's pixels ends in one of those runs.
+// Frame segments lab_link keeps in shared memory (batches of up to 128
+// frames; longer ones read them from global memory).
+constexpr int kMaxSegments = 129;
+
 __global__ void __launch_bounds__(kThreads) lab_link(LabArgs a) {
+  // the batch's frame segments, read once per block
+  __shared__ uint64_t sh_start[kMaxSegments], sh_count[kMaxSegments];
+  __shared__ int64_t sh_z[kMaxSegments];
   LabelScalars *sc = a.sc;
   const uint64_t carry = sc->carry_n;
   const int first_batch_seg = carry > 0 ? 1 : 0;
   const uint32_t W = static_cast<uint32_t>(a.width);
-  const int64_t z0 = sc->batch_z0;
   const uint32_t nruns = sc->runs_n;
+  const int nseg = static_cast<int>(sc->nseg);
+  const bool in_shared = nseg <= kMaxSegments;
+  if (in_shared)
+    for (int k = threadIdx.x; k < nseg; k += blockDim.x) {
+      sh_start[k] = a.seg_start[k];
+      sh_count[k] = a.seg_count[k];
+      sh_z[k] = a.seg_z[k];
+    }
+  __syncthreads();
+  const uint64_t *seg_start = in_shared ? sh_start : a.seg_start;
+  const uint64_t *seg_count = in_shared ? sh_count : a.seg_count;
+  const int64_t *seg_z = in_shared ? sh_z : a.seg_z;
   const int lane = threadIdx.x & 31;
   // one entry of lab_gather's list per lane, so the lanes of a warp all
   // have a run to link; a warp takes the next 32 entries when its last are
@@ -407,28 +432,26 @@ __global__ void __launch_bounds__(kThreads) lab_link(LabArgs a) {
     const uint64_t i = base + static_cast<uint64_t>(lane);
     if (i >= nruns)
       continue;
-    const uint64_t e = a.runs[i];
-    const uint64_t g = e & 0xffffffffu;
-    const uint32_t len = static_cast<uint32_t>(e >> 32) & 0x3fu;
-    uint32_t ra = static_cast<uint32_t>(g);
-    if (e >> 40) // a run crossing into a new chunk: join the pieces
-      ra = uf_unite(a.par, ra, static_cast<uint32_t>(g - 1));
-    // the batch's frames are consecutive: a new pixel's frame is its segment
-    const int s = first_batch_seg + static_cast<int>(a.fr[g] - z0);
-    const uint64_t s0 = a.seg_start[s];
-    const uint64_t end = s0 + a.seg_count[s];
-    const uint32_t idx = a.ix[g];
+    const uint4 e = a.runs[i];
+    const uint32_t g = e.x, idx = e.y;
+    const uint32_t len = e.z & 0x3fu;
+    const int s = static_cast<int>(e.z >> 8);
+    uint32_t ra = g;
+    if (e.z & 0x40u) // a run crossing into a new chunk: join the pieces
+      ra = uf_unite(a.par, ra, g - 1);
+    const uint64_t s0 = seg_start[s];
+    const uint64_t end = s0 + seg_count[s];
     const uint32_t last = idx + len - 1; // the piece's last index (one row, one chunk)
     const bool up = idx >= W;
-    const bool prev = !a.two_d && s > 0 && a.seg_z[s - 1] + 1 == a.seg_z[s];
+    const bool prev = !a.two_d && s > 0 && seg_z[s - 1] + 1 == seg_z[s];
     // both lookups' first loads before either walk
     const uint32_t tu = up ? table_of(a, s, first_batch_seg)[(idx - W) >> kBlockShift] : kNone;
     const uint32_t tp = prev ? table_of(a, s - 1, first_batch_seg)[idx >> kBlockShift] : kNone;
     const uint64_t qu = up ? first_at_least(a, tu, s0, end - s0, idx - W) : end - s0;
     uint64_t ps0 = 0, pcount = 0, qp = 0;
     if (prev) {
-      ps0 = a.seg_start[s - 1];
-      pcount = a.seg_count[s - 1];
+      ps0 = seg_start[s - 1];
+      pcount = seg_count[s - 1];
       qp = first_at_least(a, tp, ps0, pcount, idx);
     }
     if (up)

@@ -137,7 +137,7 @@ private:
   uint32_t *flist_ = nullptr;                   // the finished roots in position order
   uint32_t *comp_root_ = nullptr, *msize_ = nullptr, *members_ = nullptr;
   uint64_t *mpk_ = nullptr; // member offset (low 32) | size-filtered index (high 32)
-  uint64_t *runs_ = nullptr; // lab_link's work list
+  uint4 *runs_ = nullptr; // lab_link's work list
   uint32_t *run_starts_ = nullptr; // per 32 positions: the run starts (lab_gather)
   Spot *spot_tmp_ = nullptr;  // spots by size-filtered index, before acceptance
   Pixel *pix_tmp_ = nullptr;  // their pixels, by member offset
