@@ -102,6 +102,7 @@ SIGNATURES = {
     "sf_server_stats": (_I, [_P, _I, _P, _P]),
     "sf_server_spots": (_I, [_P, _I, _P, _S, ctypes.POINTER(_S)]),
     "sf_server_pixels": (_I, [_P, _I, _P, _S, ctypes.POINTER(_S)]),
+    "sf_server_take": (_I, [_P, _I, _P, _S, ctypes.POINTER(_S), _P, _S, ctypes.POINTER(_S)]),
     "sf_server_signal_counts": (_I, [_P, _I, _P, _S, ctypes.POINTER(_S)]),
     "sf_server_latencies": (_I, [_P, _I, _I, _P, _S, ctypes.POINTER(_S)]),
     "sf_engine_create": (_I, [_I, _I, _P, _P, _P, ctypes.POINTER(_P)]),

@@ -26,14 +26,15 @@
 //             position
 //   rank      each finished component's emission rank; size filters
 //   scan      member offsets of the components that pass the size filters
-//   scatter   members, in any order; each pixel's open flag (its component
-//             is not finished)
+//   scatter   members, in any order; the open pixels (their component is
+//             not finished) as a bitmap with a count per 32 positions
 //   accept    per component: members sorted by position (so (frame, index)
 //             order), then the FP64 pass in that order, peak-centroid
 //             filter
 //   scan      output rows and pixel offsets of the accepted spots
 //   write     spots and their pixels
-//   scan/carry  the open components' pixels compacted, in order, into
+//   scan      of the open counts
+//   carry     the open components' pixels compacted, in order, into
 //             the other live buffer and re-rooted at their first pixel
 //   finalize  running counts and the carry for the next batch
 //
@@ -84,7 +85,7 @@ struct LabArgs {
   Spot *spot_tmp;
   Pixel *pix_tmp;
   uint64_t *pack;
-  uint32_t *open;
+  uint32_t *obits, *ocnt; // open pixels: bitmap and (scanned) count per 32 positions
   uint32_t *big; // ranks of the kept components with more than kSmallCap members
   Spot *spots;
   Pixel *kept;
@@ -586,8 +587,8 @@ __global__ void __launch_bounds__(kThreads) lab_rank(LabArgs a) {
     atomicAdd(reinterpret_cast<unsigned long long *>(&sc->too_large), large);
 }
 
-// Member lists, and the open flags of every pixel (its component is not
-// finished by this batch, so it is carried). A warp takes 32 consecutive
+// Member lists, and the open pixels (their component is not finished by
+// this batch, so they are carried) as a bitmap and count per 32 positions. A warp takes 32 consecutive
 // positions; the lanes of one component claim their slots with one atomic
 // and fill them in lane order.
 // So each component's list is a set of runs, one per 32-position chunk it
@@ -600,13 +601,18 @@ __global__ void __launch_bounds__(kThreads) lab_scatter(LabArgs a) {
   for (uint64_t base = (gtid() >> 5) * 32; base < n; base += warps * 32) {
     const uint64_t g = base + lane;
     uint32_t r = kNone, rank = kNone;
+    bool open = false;
     if (g < n) {
       r = a.root[g];
       rank = a.rank_of_root[r];
-      // a pixel of a component not finished by this batch is carried
-      a.open[g] = rank == kNone ? 1u : 0u;
+      open = rank == kNone; // not finished by this batch: carried
       if (rank != kNone && a.msize[rank] == 0)
         rank = kNone;
+    }
+    const uint32_t ob = __ballot_sync(kFull, open);
+    if (lane == 0) {
+      a.obits[base >> 5] = ob;
+      a.ocnt[base >> 5] = __popc(ob);
     }
     const uint32_t key = rank == kNone ? kNone : r;
     const uint32_t peers = __match_any_sync(kFull, key);
@@ -1193,23 +1199,31 @@ __global__ void __launch_bounds__(kThreads) lab_write(LabArgs a) {
 }
 
 
-// The open pixels to the other live buffer, in order. `open` holds the
-// exclusive scan of lab_scatter's open flags, so a pixel is open where the
-// scan steps up after it (the total after the last pixel).
+// Where an open pixel lands in the carry: the scanned count of open pixels
+// in the 32-position words before its own, plus the open ones before it in
+// its word.
+__device__ __forceinline__ uint32_t open_position(const LabArgs &a, uint64_t g) {
+  return a.ocnt[g >> 5] + __popc(a.obits[g >> 5] & ((1u << (g & 31)) - 1u));
+}
+
+// The open pixels to the other live buffer, in order, a warp per
+// 32-position word (most words hold none).
 __global__ void __launch_bounds__(kThreads) lab_carry(LabArgs a) {
   LabelScalars *sc = a.sc;
-  const uint64_t n = sc->n;
-  const uint32_t total = sc->open32;
-  for (uint64_t g = gtid(); g < n; g += gstride()) {
-    const uint32_t at = a.open[g];
-    const uint32_t next = g + 1 < n ? a.open[g + 1] : total;
-    if (next == at)
+  const uint64_t nw = sc->nw;
+  const int lane = threadIdx.x & 31;
+  const uint64_t warps = gstride() >> 5;
+  for (uint64_t w = gtid() >> 5; w < nw; w += warps) {
+    const uint32_t bits = a.obits[w];
+    if (!((bits >> lane) & 1u))
       continue;
+    const uint64_t g = w * 32 + static_cast<uint64_t>(lane);
+    const uint32_t at = a.ocnt[w] + __popc(bits & ((1u << lane) - 1u));
     const uint32_t r = a.root[g];
     a.nfr[at] = a.fr[g];
     a.nix[at] = a.ix[g];
     a.nval[at] = a.val[g];
-    a.npar[at] = a.open[r]; // the root is open too, and comes first
+    a.npar[at] = open_position(a, r); // the root is open too, and comes first
   }
 }
 
@@ -1229,8 +1243,8 @@ __global__ void lab_finalize(LabArgs a) {
   sc->carry_last_z = last_batch_frame(a);
   // Every pixel of the last frame stays open (its components can still
   // grow), so the carry's last frame starts where that frame's first pixel
-  // lands: its exclusive-scan value.
-  sc->carry_last_start = sc->carry_n > 0 ? a.open[a.seg_start[sc->nseg - 1]] : 0;
+  // lands (with anything carried, the last frame has pixels).
+  sc->carry_last_start = sc->carry_n > 0 ? open_position(a, a.seg_start[sc->nseg - 1]) : 0;
   sc->batch_z0 += a.nframes;
 }
 
@@ -1288,14 +1302,14 @@ void DeviceLabeller::release() {
     l = Live();
   }
   void *ptrs[] = {root_, size_, rank_of_root_, cursor_, lastz_, bits_, bcnt_, flist_, comp_root_,
-                  msize_, mpk_, runs_, run_starts_, spot_tmp_, pix_tmp_, members_, pack_, open_, spots_out_, kept_out_, seg_start_,
+                  msize_, mpk_, runs_, run_starts_, spot_tmp_, pix_tmp_, members_, pack_, obits_, ocnt_, spots_out_, kept_out_, seg_start_,
                   seg_count_, seg_z_, tab_, big_};
   for (void *p : ptrs)
     cudaFree(p);
   tab_ = nullptr;
   root_ = size_ = rank_of_root_ = cursor_ = nullptr;
   lastz_ = nullptr;
-  bits_ = bcnt_ = flist_ = comp_root_ = msize_ = members_ = open_ = big_ = nullptr;
+  bits_ = bcnt_ = flist_ = comp_root_ = msize_ = members_ = obits_ = ocnt_ = big_ = nullptr;
   mpk_ = pack_ = nullptr;
   runs_ = nullptr;
   run_starts_ = nullptr;
@@ -1358,7 +1372,8 @@ void DeviceLabeller::reserve(uint64_t batch_pixels, int max_frames, uint64_t car
     alloc(&run_starts_, live / 32 + 1, "run starts");
     alloc(&members_, live, "members");
     alloc(&pack_, live, "spot offsets");
-    alloc(&open_, live, "open flags");
+    alloc(&obits_, nwmax, "open bitmap");
+    alloc(&ocnt_, nwmax, "open counts");
     alloc(&big_, live / (kSmallCap + 1) + 1, "large components");
     alloc(&spots_out_, spot_cap, "spots");
     alloc(&spot_tmp_, spot_cap, "spot scratch");
@@ -1448,7 +1463,8 @@ void DeviceLabeller::enqueue(int nframes, const SignalPixel *lists, const uint64
   a.pix_tmp = pix_tmp_;
   a.members = members_;
   a.pack = pack_;
-  a.open = open_;
+  a.obits = obits_;
+  a.ocnt = ocnt_;
   a.big = big_;
   a.spots = spots_out_;
   a.kept = kept_out_;
@@ -1491,7 +1507,7 @@ void DeviceLabeller::enqueue(int nframes, const SignalPixel *lists, const uint64
   check(cudaStreamWaitEvent(s, join_, 0), "cudaStreamWaitEvent");
   scan64_.run(pack_, pack_, &sc->closed, 1, live_cap_, &sc->accepted_pack, s);
   lab_write<<<grid, kThreads, 0, s>>>(a);
-  scan32_.run(open_, open_, &sc->n, 1, live_cap_, &sc->open32, s);
+  scan32_.run(ocnt_, ocnt_, &sc->nw, 1, nwmax, &sc->open32, s);
   lab_carry<<<grid, kThreads, 0, s>>>(a);
   lab_finalize<<<1, 32, 0, s>>>(a);
   check(cudaGetLastError(), "launching the labeller");

@@ -632,6 +632,34 @@ int sf_server_pixels(sf_server *server, int series, sf_pixel *out, size_t capaci
   });
 }
 
+int sf_server_take(sf_server *server, int series, sf_spot *spots, size_t spot_capacity,
+                   size_t *nspots, sf_pixel *pixels, size_t pixel_capacity, size_t *npixels) {
+  return guarded([&] {
+    if (!server || !nspots || !npixels)
+      return -1;
+    ServerSeries &se = reinterpret_cast<Server *>(server)->at(series);
+    std::lock_guard<std::mutex> g(se.m);
+    // a run's spot block and pixel block are pushed together (a spot has
+    // pixels), so the blocks pair up; take whole runs while both fit
+    size_t ns = 0, np = 0, k = 0;
+    while (k < se.spots.size() && k < se.pixels.size() &&
+           ns + se.spots[k].size() <= spot_capacity && np + se.pixels[k].size() <= pixel_capacity) {
+      if (!se.spots[k].empty())
+        std::memcpy(spots + ns, se.spots[k].data(), se.spots[k].size() * sizeof(sf::Spot));
+      if (!se.pixels[k].empty())
+        std::memcpy(pixels + np, se.pixels[k].data(), se.pixels[k].size() * sizeof(sf::Pixel));
+      ns += se.spots[k].size();
+      np += se.pixels[k].size();
+      k++;
+    }
+    se.spots.erase(se.spots.begin(), se.spots.begin() + k);
+    se.pixels.erase(se.pixels.begin(), se.pixels.begin() + k);
+    *nspots = ns;
+    *npixels = np;
+    return (k == 0 && !se.spots.empty()) ? -2 : 0;
+  });
+}
+
 int sf_server_signal_counts(sf_server *server, int series, uint32_t *out, size_t capacity,
                             size_t *n) {
   return guarded([&] {

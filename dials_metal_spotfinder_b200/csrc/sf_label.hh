@@ -142,7 +142,7 @@ private:
   Spot *spot_tmp_ = nullptr;  // spots by size-filtered index, before acceptance
   Pixel *pix_tmp_ = nullptr;  // their pixels, by member offset
   uint64_t *pack_ = nullptr;
-  uint32_t *open_ = nullptr;
+  uint32_t *obits_ = nullptr, *ocnt_ = nullptr; // open pixels per 32 positions
   uint32_t *big_ = nullptr; // ranks of the components lab_accept's large launch takes
   Spot *spots_out_ = nullptr;
   Pixel *kept_out_ = nullptr;

@@ -101,6 +101,21 @@ class Server:
     def pixels(self, series: int) -> np.ndarray:
         return self._array(lib.sf_server_pixels, series, PIXEL)
 
+    def take(self, series: int, spot_capacity: int = 1 << 18, pixel_capacity: int = 1 << 24,
+             out=None):
+        """The spots (and their pixels) finished so far and still held, which
+        the series then forgets (sf_server_take): call it as results are
+        consumed so a long series does not hold every spot in host memory.
+        `out` = (spot array, pixel array) to fill; returns views of the
+        filled parts."""
+        if out is None:
+            out = (np.zeros(spot_capacity, SPOT), np.zeros(pixel_capacity, PIXEL))
+        sp, px = out
+        ns, npx = ctypes.c_size_t(0), ctypes.c_size_t(0)
+        raise_for(lib.sf_server_take(self._h, series, sp.ctypes.data, len(sp), ctypes.byref(ns),
+                                     px.ctypes.data, len(px), ctypes.byref(npx)), "sf_server_take")
+        return sp[: ns.value], px[: npx.value]
+
     def signal_counts(self, series: int) -> np.ndarray:
         return self._array(lib.sf_server_signal_counts, series, np.uint32)
 
@@ -149,18 +164,43 @@ class _NoGc:
             gc.enable()
 
 
-def drive(streams, hbm_budget=0, slots=3, use_graph=True):
+def drive(streams, hbm_budget=0, slots=3, use_graph=True, drain_s=0.05):
     """Replays every stream on its own thread at its frame rate through one
-    Server and returns per-stream results (latencies in ms)."""
+    Server and returns per-stream results (latencies in ms). A consumer
+    thread per stream takes the finished spots every `drain_s` seconds (as
+    a live writer of the reflection table would), so the series do not hold
+    a whole acquisition's spots in host memory."""
     with _NoGc():
-        return _drive(streams, hbm_budget, slots, use_graph)
+        return _drive(streams, hbm_budget, slots, use_graph, drain_s)
 
 
-def _drive(streams, hbm_budget, slots, use_graph):
+def _drive(streams, hbm_budget, slots, use_graph, drain_s):
     out = []
     with Server(hbm_budget=hbm_budget, slots=slots, use_graph=use_graph) as srv:
         ids = [srv.open(s.shape, two_d=s.two_d) for s in streams]
         late = [0] * len(streams)
+        taken = [[0, 0] for _ in streams]
+        running = threading.Event()
+        running.set()
+        bufs = [(np.zeros(1 << 18, SPOT), np.zeros(1 << 24, PIXEL)) for _ in streams]
+
+        def consume(k):
+            while True:
+                stop = not running.is_set()
+                while True:
+                    sp, px = srv.take(ids[k], out=bufs[k])
+                    taken[k][0] += len(sp)
+                    taken[k][1] += len(px)
+                    if len(sp) == 0:
+                        break
+                if stop:
+                    return
+                time.sleep(drain_s)
+
+        consumers = [threading.Thread(target=consume, args=(k,)) for k in range(len(streams))]
+        if drain_s:
+            for t in consumers:
+                t.start()
         t0 = time.perf_counter() + 0.05
 
         def produce(k):
@@ -183,8 +223,13 @@ def _drive(streams, hbm_budget, slots, use_graph):
         for t in threads:
             t.join()
         wall = time.perf_counter() - t0
-        for k, s in enumerate(streams):
+        for k in range(len(streams)):
             srv.finish(ids[k])
+        running.clear()
+        if drain_s:
+            for t in consumers:
+                t.join()
+        for k, s in enumerate(streams):
             st = srv.stats(ids[k])
             out.append({
                 "shape": list(s.shape), "rate_hz": s.rate_hz, "frames": s.frames,
@@ -196,7 +241,8 @@ def _drive(streams, hbm_budget, slots, use_graph):
                                         percentiles(srv.latencies_us(ids[k], "grouped")).items()},
                 "frame_to_spot_ms": {k2: (v / 1e3 if v is not None else None) for k2, v in
                                      percentiles(srv.latencies_us(ids[k], "spot")).items()},
-                "spots": int(st["accepted"]), "device_bytes": st["device_bytes"],
+                "spots": int(st["accepted"]), "spots_taken_live": taken[k][0],
+                "device_bytes": st["device_bytes"],
             })
     return out
 

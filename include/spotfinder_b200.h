@@ -428,6 +428,18 @@ SF_API int sf_server_spots(sf_server *server, int series, sf_spot *out, size_t c
                            size_t *n);
 SF_API int sf_server_pixels(sf_server *server, int series, sf_pixel *out, size_t capacity,
                             size_t *n);
+/* Takes the spots (and their pixels) finished so far and still held, in
+ * order, whole runs at a time while both arrays have room, and lets the
+ * series forget them: a live consumer (writing a reflection table, say)
+ * calls this as it goes, so the series does not keep every spot of a long
+ * acquisition in host memory. A spot's `first` stays the offset of its
+ * pixels in the series' whole pixel sequence, taken or not. -2 if the first
+ * held run does not fit (nothing taken). sf_server_spots and
+ * sf_server_pixels return what is still held. The reference's series
+ * consumer writes the table at the end (src/find_spots.cc:636-716). */
+SF_API int sf_server_take(sf_server *server, int series, sf_spot *spots, size_t spot_capacity,
+                          size_t *nspots, sf_pixel *pixels, size_t pixel_capacity,
+                          size_t *npixels);
 /* Signal pixels per frame, by frame number (0 for a dropped frame). */
 SF_API int sf_server_signal_counts(sf_server *server, int series, uint32_t *out,
                                    size_t capacity, size_t *n);

@@ -147,3 +147,34 @@ def test_u32_series_served(gpu_lib):
         srv.finish(sid)
         got = results(srv, sid)
     check_oracle(frames, False, *got)
+
+
+def test_take_as_results_arrive(gpu_lib):
+    """take() while frames are still being submitted, and once more after
+    the close: the pieces, in order, are the oracle's spots and pixels, and
+    what the series still holds afterwards is nothing; a spot array too
+    short for the first held run takes nothing (Overflow)."""
+    import dials_metal_spotfinder_b200 as sf
+    from dials_metal_spotfinder_b200.serve import Server
+    s, frames, two_d = series_a()
+    chunks = encode_all(frames)
+    got_spots, got_pixels = [], []
+    with Server() as srv:
+        sid = srv.open(frames[0].shape, two_d=two_d)
+        for i, c in enumerate(chunks):
+            assert srv.submit(sid, c, timeout_s=30)
+            if i % 3 == 2:
+                sp, px = srv.take(sid)
+                got_spots.append(sp.copy())
+                got_pixels.append(px.copy())
+        srv.finish(sid)
+        held = srv.spots(sid)
+        if len(held):
+            with pytest.raises(sf.Overflow):
+                srv.take(sid, spot_capacity=0)
+        sp, px = srv.take(sid)
+        got_spots.append(sp.copy())
+        got_pixels.append(px.copy())
+        assert len(srv.spots(sid)) == 0 and len(srv.pixels(sid)) == 0
+        st, counts = srv.stats(sid), srv.signal_counts(sid)
+    check_oracle(frames, two_d, np.concatenate(got_spots), np.concatenate(got_pixels), st, counts)
