@@ -159,7 +159,7 @@ class TuneOptions(ctypes.Structure):
 class TuneResult(ctypes.Structure):
     _fields_ = [("frames_per_launch", ctypes.c_int32), ("warps_per_block", ctypes.c_int32),
                 ("seg_rows", ctypes.c_int32), ("from_cache", ctypes.c_int32),
-                ("candidates", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("candidates", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
                 ("seg_ratio", ctypes.c_double), ("us_per_frame", ctypes.c_double)]
 
     def as_dict(self) -> dict:

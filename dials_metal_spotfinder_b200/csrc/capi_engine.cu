@@ -91,7 +91,9 @@ int sf_engine_create(int elem_bytes, int nframes, const int32_t *heights,
                                             nullptr, &tuned);
     if (from_cache) {
       t.warps_per_block = tuned.warps_per_block;
-      t.seg_rows = sf::tune_seg_rows(elem_bytes, shapes, tuned.warps_per_block, tuned.seg_ratio);
+      t.blocks_per_sm = tuned.blocks_per_sm;
+      t.seg_rows = sf::tune_seg_rows(elem_bytes, shapes, tuned.warps_per_block, tuned.seg_ratio,
+                                     tuned.blocks_per_sm);
     }
     auto e = sf::make_engine(elem_bytes, shapes, t, slots);
     e->tuned_from_cache = from_cache;
@@ -111,6 +113,7 @@ int sf_engine_tuning(sf_engine *engine, sf_tune_result *out) {
     out->frames_per_launch = e->plan->nframes();
     out->warps_per_block = e->plan->tuning().warps_per_block;
     out->seg_rows = e->plan->tuning().seg_rows;
+    out->blocks_per_sm = e->plan->tuning().blocks_per_sm;
     out->from_cache = e->tuned_from_cache ? 1 : 0;
     return 0;
   });

@@ -62,11 +62,14 @@ int choose_seg_rows(const std::vector<ThresholdPlan::Shape> &shapes, uint64_t re
 
 } // namespace
 
-int model_seg_rows(int elem_bytes, const std::vector<ThresholdPlan::Shape> &shapes, int wpc) {
-  const int occ = elem_bytes == 2 ? threshold_occupancy<uint16_t>(wpc)
-                                  : threshold_occupancy<uint32_t>(wpc);
+int model_seg_rows(int elem_bytes, const std::vector<ThresholdPlan::Shape> &shapes, int wpc,
+                   int blocks_per_sm) {
+  int occ = elem_bytes == 2 ? threshold_occupancy<uint16_t>(wpc)
+                            : threshold_occupancy<uint32_t>(wpc);
   if (occ < 1)
     throw DeviceError("the threshold kernel does not fit on this device");
+  if (blocks_per_sm > 0)
+    occ = std::min(occ, blocks_per_sm);
   return choose_seg_rows(shapes, static_cast<uint64_t>(device_sm_count()) * occ * wpc);
 }
 

@@ -25,6 +25,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <iterator>
 #include <mutex>
 #include <thread>
 
@@ -638,25 +639,43 @@ int sf_server_take(sf_server *server, int series, sf_spot *spots, size_t spot_ca
     if (!server || !nspots || !npixels)
       return -1;
     ServerSeries &se = reinterpret_cast<Server *>(server)->at(series);
-    std::lock_guard<std::mutex> g(se.m);
     // a run's spot block and pixel block are pushed together (a spot has
-    // pixels), so the blocks pair up; take whole runs while both fit
-    size_t ns = 0, np = 0, k = 0;
-    while (k < se.spots.size() && k < se.pixels.size() &&
-           ns + se.spots[k].size() <= spot_capacity && np + se.pixels[k].size() <= pixel_capacity) {
-      if (!se.spots[k].empty())
-        std::memcpy(spots + ns, se.spots[k].data(), se.spots[k].size() * sizeof(sf::Spot));
-      if (!se.pixels[k].empty())
-        std::memcpy(pixels + np, se.pixels[k].data(), se.pixels[k].size() * sizeof(sf::Pixel));
-      ns += se.spots[k].size();
-      np += se.pixels[k].size();
-      k++;
+    // pixels), so the blocks pair up; take whole runs while both fit. The
+    // blocks are moved out under the series' lock and copied after it, so
+    // the series' submits and collector do not wait on the copy.
+    std::vector<std::vector<sf::Spot>> sp;
+    std::vector<std::vector<sf::Pixel>> px;
+    bool none_fit = false;
+    {
+      std::lock_guard<std::mutex> g(se.m);
+      size_t ns = 0, np = 0, k = 0;
+      while (k < se.spots.size() && k < se.pixels.size() &&
+             ns + se.spots[k].size() <= spot_capacity &&
+             np + se.pixels[k].size() <= pixel_capacity) {
+        ns += se.spots[k].size();
+        np += se.pixels[k].size();
+        k++;
+      }
+      none_fit = k == 0 && !se.spots.empty();
+      sp.assign(std::make_move_iterator(se.spots.begin()),
+                std::make_move_iterator(se.spots.begin() + k));
+      px.assign(std::make_move_iterator(se.pixels.begin()),
+                std::make_move_iterator(se.pixels.begin() + k));
+      se.spots.erase(se.spots.begin(), se.spots.begin() + k);
+      se.pixels.erase(se.pixels.begin(), se.pixels.begin() + k);
     }
-    se.spots.erase(se.spots.begin(), se.spots.begin() + k);
-    se.pixels.erase(se.pixels.begin(), se.pixels.begin() + k);
+    size_t ns = 0, np = 0;
+    for (size_t k = 0; k < sp.size(); k++) {
+      if (!sp[k].empty())
+        std::memcpy(spots + ns, sp[k].data(), sp[k].size() * sizeof(sf::Spot));
+      if (!px[k].empty())
+        std::memcpy(pixels + np, px[k].data(), px[k].size() * sizeof(sf::Pixel));
+      ns += sp[k].size();
+      np += px[k].size();
+    }
     *nspots = ns;
     *npixels = np;
-    return (k == 0 && !se.spots.empty()) ? -2 : 0;
+    return none_fit ? -2 : 0;
   });
 }
 

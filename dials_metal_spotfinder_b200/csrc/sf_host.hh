@@ -171,7 +171,8 @@ private:
 
 // The cost model's task height (plan.cu) for these shapes at `wpc` warps per
 // block and as many blocks per SM as fit.
-int model_seg_rows(int elem_bytes, const std::vector<ThresholdPlan::Shape> &shapes, int wpc);
+int model_seg_rows(int elem_bytes, const std::vector<ThresholdPlan::Shape> &shapes, int wpc,
+                   int blocks_per_sm = 0);
 
 // The autotuner (tune.cu). An entry is what a search measured best for one
 // frame shape on one kind of device: frames per launch, warps per block, the
@@ -181,6 +182,7 @@ struct TuneEntry {
   int warps_per_block = 2;
   double seg_ratio = 1.0;
   double us_per_frame = 0.0;
+  int blocks_per_sm = 0; // threshold blocks per SM; 0: as many as fit
 };
 struct TuneOptions {
   int min_frames = 8, max_frames = 32, steps = 4;
@@ -196,7 +198,7 @@ struct TuneResult {
 std::string tune_cache_path(const char *given);
 bool tune_lookup(int elem_bytes, int height, int width, const char *cache_path, TuneEntry *out);
 int tune_seg_rows(int elem_bytes, const std::vector<ThresholdPlan::Shape> &shapes, int wpc,
-                  double ratio);
+                  double ratio, int blocks_per_sm = 0);
 TuneResult tune_search(int elem_bytes, int height, int width, const void *const *sample,
                        int nsample, const TuneOptions &options);
 

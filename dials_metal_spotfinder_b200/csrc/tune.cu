@@ -13,7 +13,11 @@
 //      ratio to it, so the choice carries over to other batch sizes);
 //   2. the whole step, threshold + placement + 3D grouping on two slots as
 //      the engine overlaps them, for each frames-per-launch candidate within
-//      the caller's range, using the best ratio and warps from step 1.
+//      the caller's range, using the best ratio and warps from step 1;
+//   3. at the best batch size, fewer threshold blocks per SM than fit: the
+//      threshold then leaves registers and warp slots on every SM for the
+//      previous batch's grouping kernels, which run beside it on the other
+//      stream, instead of holding them until it ends.
 //
 // The tuner file holds one line per (pixel bytes, height, width, SM count,
 // device name): frames per launch, warps per block, the task-height ratio,
@@ -76,6 +80,8 @@ bool read_entry(const std::string &path, const std::string &key, TuneEntry *out)
     TuneEntry e;
     if (!(ls >> k >> e.frames >> e.warps_per_block >> e.seg_ratio >> e.us_per_frame))
       continue;
+    if (!(ls >> e.blocks_per_sm) || e.blocks_per_sm < 0)
+      e.blocks_per_sm = 0;
     if (k != key || e.frames < 1 || e.seg_ratio <= 0 ||
         (e.warps_per_block != 1 && e.warps_per_block != 2 && e.warps_per_block != 4))
       continue;
@@ -91,7 +97,7 @@ void append_entry(const std::string &path, const std::string &key, const TuneEnt
   if (!o)
     return; // a read-only location: the result is still returned
   o << key << " " << e.frames << " " << e.warps_per_block << " " << e.seg_ratio << " "
-    << e.us_per_frame << "\n";
+    << e.us_per_frame << " " << e.blocks_per_sm << "\n";
 }
 
 // Milliseconds per frame of `steps` runs of an engine built for F frames of
@@ -152,8 +158,8 @@ bool tune_lookup(int elem_bytes, int height, int width, const char *cache_path,
 }
 
 int tune_seg_rows(int elem_bytes, const std::vector<ThresholdPlan::Shape> &shapes, int wpc,
-                  double ratio) {
-  const int base = model_seg_rows(elem_bytes, shapes, wpc);
+                  double ratio, int blocks_per_sm) {
+  const int base = model_seg_rows(elem_bytes, shapes, wpc, blocks_per_sm);
   int max_h = 1;
   for (const auto &s : shapes)
     max_h = std::max(max_h, s.height);
@@ -231,7 +237,32 @@ TuneResult tune_search(int elem_bytes, int height, int width, const void *const 
     best_f = F1;
     best2 = best1;
   }
+  // 3. threshold blocks per SM at that batch size
+  int best_bps = 0;
+  {
+    const int occ = elem_bytes == 2 ? threshold_occupancy<uint16_t>(best_wpc)
+                                    : threshold_occupancy<uint32_t>(best_wpc);
+    const std::vector<ThresholdPlan::Shape> shapes(best_f, ThresholdPlan::Shape{height, width});
+    int last = occ;
+    for (int bps : {occ - 1, (3 * occ) / 4, occ / 2}) {
+      if (bps < 1 || bps >= last)
+        continue;
+      last = bps;
+      PlanTuning t;
+      t.warps_per_block = best_wpc;
+      t.blocks_per_sm = bps;
+      t.seg_rows = tune_seg_rows(elem_bytes, shapes, best_wpc, best_ratio, bps);
+      const double ms = time_engine(elem_bytes, height, width, best_f, t, o.grouping, sample,
+                                    nsample, o.steps);
+      r.candidates++;
+      if (ms < best2) {
+        best2 = ms;
+        best_bps = bps;
+      }
+    }
+  }
   r.entry.frames = best_f;
+  r.entry.blocks_per_sm = best_bps;
   r.entry.warps_per_block = best_wpc;
   r.entry.seg_ratio = best_ratio;
   r.entry.us_per_frame = 1000.0 * best2;
@@ -272,7 +303,8 @@ extern "C" int sf_tune(int elem_bytes, int height, int width, const void *const 
     out->frames_per_launch = r.entry.frames;
     out->warps_per_block = r.entry.warps_per_block;
     out->seg_rows = sf::tune_seg_rows(elem_bytes, shapes, r.entry.warps_per_block,
-                                      r.entry.seg_ratio);
+                                      r.entry.seg_ratio, r.entry.blocks_per_sm);
+    out->blocks_per_sm = r.entry.blocks_per_sm;
     out->from_cache = r.from_cache ? 1 : 0;
     out->candidates = r.candidates;
     out->seg_ratio = r.entry.seg_ratio;

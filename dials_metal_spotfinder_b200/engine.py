@@ -70,7 +70,7 @@ class Engine:
         d = out.as_dict()
         d["from_cache"] = bool(d["from_cache"])
         return {k: d[k] for k in ("frames_per_launch", "warps_per_block", "seg_rows",
-                                  "from_cache")}
+                                  "blocks_per_sm", "from_cache")}
 
     def upload(self, slot: int, frame: int, image: np.ndarray) -> None:
         """Asynchronous host-to-device copy; keep `image` alive (and unchanged)

@@ -315,7 +315,9 @@ SF_API int sf_engine_stage_totals(sf_engine *engine, double out4[4]);
  * A timed search for one frame shape on the current device: warps per block
  * x threshold task height (threshold alone), then frames per launch
  * (threshold + placement + 3D grouping, two slots, as the engine overlaps
- * them), on the caller's sample frames (host, row-major, cycled into the
+ * them), then threshold blocks per SM at that batch size (fewer than fit
+ * leave room on every SM for the grouping running beside it), on the
+ * caller's sample frames (host, row-major, cycled into the
  * batches), with CUDA events. The best tuple is appended to a tuner file,
  * keyed by pixel type, shape, SM count and device name; engines created
  * without explicit tuning read it. Results never depend on the tuning, only
@@ -339,7 +341,7 @@ typedef struct sf_tune_result {
   int32_t seg_rows;       /* for frames_per_launch frames */
   int32_t from_cache;     /* 1: read from the tuner file, no search */
   int32_t candidates;     /* configurations timed */
-  int32_t reserved;
+  int32_t blocks_per_sm;  /* threshold blocks per SM; 0 = as many as fit */
   double seg_ratio;       /* task height / the cost model's */
   double us_per_frame;    /* the chosen tuple's measured time per frame */
 } sf_tune_result;

@@ -47,11 +47,13 @@ def test_search_cache_and_engine_default(gpu_lib, tmp_path, monkeypatch):
     first = tune(sample, min_frames=4, max_frames=8, steps=2)
     assert not first["from_cache"] and first["candidates"] >= 4
     assert first["frames_per_launch"] in (4, 8)  # the candidates inside the range
+    assert first["candidates"] >= 4
     assert first["warps_per_block"] in (1, 2, 4) and first["seg_rows"] >= 16
     assert first["us_per_frame"] > 0
     again = tune(sample, min_frames=4, max_frames=8)
     assert again["from_cache"] and again["candidates"] == 0
-    for k in ("frames_per_launch", "warps_per_block", "seg_rows", "seg_ratio"):
+    assert first["blocks_per_sm"] >= 0
+    for k in ("frames_per_launch", "warps_per_block", "seg_rows", "seg_ratio", "blocks_per_sm"):
         assert again[k] == first[k], k
 
     F = first["frames_per_launch"]
@@ -60,6 +62,7 @@ def test_search_cache_and_engine_default(gpu_lib, tmp_path, monkeypatch):
     assert tuned[0]["from_cache"]
     assert tuned[0]["warps_per_block"] == first["warps_per_block"]
     assert tuned[0]["seg_rows"] == first["seg_rows"]
+    assert tuned[0]["blocks_per_sm"] == first["blocks_per_sm"]
     other = _run(frames, F, seg_rows=17, warps_per_block=1)
     assert not other[0]["from_cache"] and other[0]["seg_rows"] == 17
     for a, b in zip(tuned[1], other[1]):
