@@ -439,22 +439,29 @@ def run_ours(args, ranks):
         def chunk_upload(slot):
             eng.upload_chunks(slot, [b.array for b in cb])
 
-        chunk_upload(0)
-        eng.run(0)
-        e2e_read()
-        eng.synchronize()
-        d2h.clear()
-        ranks.barrier()
-        t0 = time.perf_counter()
-        chunk_upload(0)
-        eng.run(0)
-        for i in range(1, args.e2e_steps):
-            chunk_upload(i % 2)
+        def chunk_upload_each(slot):
+            for f in range(F):
+                eng.upload_chunk(slot, f, cb[f].array)
+
+        def timed_chunks(upload):
+            upload(0)
+            eng.run(0)
             e2e_read()
-            eng.run(i % 2)
-        e2e_read()
-        eng.synchronize()
-        dt = ranks.max(time.perf_counter() - t0)
+            eng.synchronize()
+            d2h.clear()
+            ranks.barrier()
+            t0 = time.perf_counter()
+            upload(0)
+            eng.run(0)
+            for i in range(1, args.e2e_steps):
+                upload(i % 2)
+                e2e_read()
+                eng.run(i % 2)
+            e2e_read()
+            eng.synchronize()
+            return ranks.max(time.perf_counter() - t0)
+
+        dt = timed_chunks(chunk_upload)
         e2e_chunks = {"value": ranks.sum(F * args.e2e_steps) / dt, "unit": UNIT,
                       "h2d_bytes_per_step": chunk_bytes,
                       "d2h_bytes_per_step": int(statistics.mean(d2h)),
@@ -462,6 +469,13 @@ def run_ours(args, ranks):
                       "form": "Engine.upload_chunks of bslz4 chunks from pinned host memory "
                               "(framing checked on host threads, decoded on the device), "
                               "run, spots/pixels into pinned host arrays; pipelined as e2e"}
+        # the same steps with the chunks handed over one call each
+        # (upload_chunk), their framing walked on the calling thread: what
+        # the batched call's parallel framing walk is worth, in one run
+        dt_each = timed_chunks(chunk_upload_each)
+        e2e_chunks["one_call_per_chunk"] = {
+            "value": ranks.sum(F * args.e2e_steps) / dt_each, "unit": UNIT,
+            "form": "Engine.upload_chunk per frame, otherwise as above"}
         for b in hb + cb + [spot_buf, pix_buf]:
             b.close()
 

@@ -240,6 +240,10 @@ __global__ void lab_setup(LabArgs a) {
 // A lookup of one index is then a scan of about two entries.
 constexpr int kBlockShift = 6;
 
+// Frame segments lab_gather and lab_link keep in shared memory (batches of
+// up to 128 frames; longer ones read them from global memory).
+constexpr int kMaxSegments = 129;
+
 __device__ __forceinline__ const uint32_t *table_of(const LabArgs &a, int s, int first_batch_seg) {
   return s < first_batch_seg ? a.carry_tab : a.tab + static_cast<uint64_t>(s - first_batch_seg) * a.nblk;
 }
@@ -259,6 +263,18 @@ __global__ void __launch_bounds__(kThreads) lab_gather(LabArgs a) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   __shared__ uint32_t warp_count[kThreads / 32];
   __shared__ uint32_t block_at;
+  // the segments' starts and frame numbers, for every pixel's lookup
+  __shared__ uint64_t sh_start[kMaxSegments];
+  __shared__ int64_t sh_z[kMaxSegments];
+  const bool in_shared = nseg <= kMaxSegments;
+  if (in_shared)
+    for (int k = threadIdx.x; k < nseg; k += blockDim.x) {
+      sh_start[k] = a.seg_start[k];
+      sh_z[k] = a.seg_z[k];
+    }
+  __syncthreads();
+  const uint64_t *seg_start = in_shared ? sh_start : a.seg_start;
+  const int64_t *seg_z = in_shared ? sh_z : a.seg_z;
   // block-uniform trip count: the run list is appended to once per block
   for (uint64_t block_base = static_cast<uint64_t>(blockIdx.x) * kThreads; block_base < n;
        block_base += static_cast<uint64_t>(gridDim.x) * kThreads) {
@@ -273,13 +289,13 @@ __global__ void __launch_bounds__(kThreads) lab_gather(LabArgs a) {
       a.rank_of_root[g] = kNone;
       a.cursor[g] = 0;
       if (g >= carry) {
-        const int s = segment_of(a.seg_start, nseg, g);
+        const int s = segment_of(seg_start, nseg, g);
         seg = s;
         const int f = s - first_batch_seg;
-        const uint64_t i = g - a.seg_start[s];
+        const uint64_t i = g - seg_start[s];
         const SignalPixel *list = a.lists + a.offs[f];
         const SignalPixel px = list[i];
-        a.fr[g] = static_cast<int32_t>(a.seg_z[s]);
+        a.fr[g] = static_cast<int32_t>(seg_z[s]);
         a.ix[g] = px.index;
         a.val[g] = px.value;
         pidx = px.index;
@@ -394,10 +410,6 @@ __device__ __forceinline__ uint32_t unite_overlaps(const LabArgs &a, uint32_t ra
 // here. The first pixel of each run then unites it with every run of the row
 // above, and of the previous frame's same row, that overlaps its span: each
 // up or previous-frame edge of the run's pixels ends in one of those runs.
-// Frame segments lab_link keeps in shared memory (batches of up to 128
-// frames; longer ones read them from global memory).
-constexpr int kMaxSegments = 129;
-
 __global__ void __launch_bounds__(kThreads) lab_link(LabArgs a) {
   // the batch's frame segments, read once per block
   __shared__ uint64_t sh_start[kMaxSegments], sh_count[kMaxSegments];

@@ -44,6 +44,9 @@ def fake_engine(sf):
         def upload_chunks(self, slot, chunks, frames=None, algorithm="bslz4"):
             assert len(chunks) == len(self.shapes)
 
+        def upload_chunk(self, slot, frame, chunk, algorithm="bslz4"):
+            assert 0 <= frame < len(self.shapes)
+
         def synchronize(self):
             pass
 
