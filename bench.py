@@ -44,6 +44,11 @@ METRIC = "16M uint16 frames/s (threshold+3D label), % HBM roofline; p99 frame la
 UNIT = "frames/s"
 SHAPE = (4362, 4148)
 L2_BYTES = 126 * 1024 * 1024
+# both arms name the workload the same way
+WORKLOAD = "Eiger2-16M-shaped uint16 frames, 4362x4148, threshold + 3D grouping + spot pass"
+# frames per step when the autotuner does not choose (its range is 8-32; it
+# has chosen 32 on these frames), and the reference arm's step
+DEFAULT_FRAMES = 32
 
 
 def parse():
@@ -266,9 +271,9 @@ def run_reference_arm(args, ranks):
     if ranks.rank != 0:
         return
     threads = os.cpu_count() or 1
-    # the same frames per step as the product arm (whose autotuner picks 16
-    # on these frames; --batch fixes both arms)
-    n = args.batch or 16
+    # the same frames per step as the product arm (--batch fixes both arms;
+    # otherwise its autotuner picks, 32 on these frames)
+    n = args.batch or DEFAULT_FRAMES
     frames = make_pool(n)
     for _ in range(max(0, min(args.warmup, 1))):
         cpu_reference(frames[:2], threads)
@@ -285,8 +290,8 @@ def run_reference_arm(args, ranks):
         "n_gpus": args.gpus, "steps": len(times), "warmup": args.warmup,
         "ms_per_step": 1000 * sum(times) / len(times), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u16/f32", "data": "synthetic",
-        "config": {"workload": "16M uint16 frames, threshold + 3D grouping on the host",
-                   "frames_per_step": n, "shape": list(SHAPE)},
+        "config": {"workload": WORKLOAD, "frames_per_step": n, "shape": list(SHAPE),
+                   "where": "the reference's dext.cc + dials_spots.cc on the host cores"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
                          "sample": f"{n} frames of 4362x4148 per step"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -310,7 +315,7 @@ def run_ours(args, ranks):
         t0 = time.perf_counter()
         tuning = tune(pool[:16], min_frames=8, max_frames=32)
         tuning["seconds"] = time.perf_counter() - t0
-    F = args.batch or (tuning["frames_per_launch"] if tuning else 16)
+    F = args.batch or (tuning["frames_per_launch"] if tuning else DEFAULT_FRAMES)
     eng = Engine([SHAPE] * F, np.uint16, slots=2)
     eng.enable_grouping(first_frame=0)
     info = eng.info()
@@ -538,10 +543,10 @@ def run_ours(args, ranks):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u16 pixels, u32 sums, f32 tests, f64 spots", "data": "synthetic",
-        "config": {"workload": "Eiger2-16M-shaped uint16 frames, 4362x4148, batched engine",
+        "config": {"workload": WORKLOAD, "shape": list(SHAPE),
                    "frames_per_step": F, "slots": 2, "distinct_frames": len(pool),
-                   "pipeline": "threshold + ordered compaction + 3D grouping + spot pass",
-                   "l2": "inputs larger than L2 (580 MB per step)",
+                   "where": "the batched engine on the device",
+                   "l2": f"inputs larger than L2 ({F * frame_bytes / 1e6:.0f} MB per step)",
                    "parallelism": f"replicas x{ranks.world}",
                    "engine": info},
         "tuning": {"search": tuning, "engine": engine_tuning},

@@ -484,8 +484,10 @@ __global__ void __launch_bounds__(kThreads) lab_keep_table(LabArgs a) {
     a.carry_tab[b] = last[b];
 }
 
-// Roots, component sizes and last frames. Lanes of one warp that share a
-// root (neighbours in a run, mostly) make one update between them.
+// Roots, component sizes and last frames. A warp's lanes hold 32
+// consecutive positions; each stretch of adjacent lanes with one root (a
+// run, mostly) makes one update. Positions are in (frame, index) order, so
+// a stretch's last frame is its last lane's.
 __global__ void __launch_bounds__(kThreads) lab_flatten(LabArgs a) {
   const uint64_t n = a.sc->n;
   const int lane = threadIdx.x & 31;
@@ -499,13 +501,16 @@ __global__ void __launch_bounds__(kThreads) lab_flatten(LabArgs a) {
       a.root[g] = r;
       z = a.fr[g];
     }
-    const uint32_t peers = __match_any_sync(kFull, r);
-    int32_t zmax = z;
-    for (uint32_t m = peers & (peers - 1); m; m &= m - 1) // other lanes of the group
-      zmax = max(zmax, __shfl_sync(peers, z, __ffs(m) - 1));
-    if (r != kNone && lane == __ffs(peers) - 1) {
-      atomicAdd(&a.size[r], static_cast<uint32_t>(__popc(peers)));
-      atomicMax(&a.lastz[r], zmax);
+    const uint32_t before = __shfl_up_sync(kFull, r, 1);
+    const bool head = lane == 0 || before != r;
+    const uint32_t heads = __ballot_sync(kFull, head);
+    // the stretch ends before the next head (bits above this lane)
+    const uint32_t later = lane == 31 ? 0u : heads & (0xfffffffeu << lane);
+    const int end = later ? __ffs(later) - 2 : 31;
+    const int32_t zlast = __shfl_sync(kFull, z, end);
+    if (head && r != kNone) {
+      atomicAdd(&a.size[r], static_cast<uint32_t>(end - lane + 1));
+      atomicMax(&a.lastz[r], zlast);
     }
   }
 }

@@ -134,7 +134,7 @@ def test_bench_line_has_the_contract_keys(monkeypatch):
     e = d["e2e"]
     for key in ("value", "unit", "h2d_bytes_per_step", "d2h_bytes_per_step"):
         assert key in e, key
-    assert e["h2d_bytes_per_step"] == 16 * bench.SHAPE[0] * bench.SHAPE[1] * 2
+    assert e["h2d_bytes_per_step"] == bench.DEFAULT_FRAMES * bench.SHAPE[0] * bench.SHAPE[1] * 2
     assert e["d2h_bytes_per_step"] == 7 * sf.SPOT.itemsize + 40 * sf.PIXEL.itemsize
     assert d["gpu_launches"] > 0 and d["gpu_launches"] % d["steps"] == 0
     assert d["gpixels_per_s"] > 0 and d["pipeline_bytes"]["per_frame"] > 0
