@@ -54,7 +54,7 @@ constexpr int kThreads = 256;
 // Components up to this many members take lab_accept's launch with small
 // per-warp buffers (many warps per SM); the few larger ones are listed by
 // lab_rank and taken by a second launch with large buffers.
-constexpr uint32_t kSmallCap = 512;
+constexpr uint32_t kSmallCap = 256;
 
 struct LabArgs {
   int32_t width;
@@ -1108,7 +1108,7 @@ __device__ bool spot_pass_warp(uint32_t W, double max_sep, const WarpBuffers &b,
 // With `listed`, the components are lab_rank's list of the large ones
 // rather than every finished root.
 template <uint32_t CAP>
-__global__ void __launch_bounds__(kCompWarps * 32) lab_accept(LabArgs a, uint32_t lo,
+__global__ void __launch_bounds__(kCompWarps * 32, CAP <= 256 ? 8 : 1) lab_accept(LabArgs a, uint32_t lo,
                                                               uint32_t hi, int listed) {
   extern __shared__ __align__(16) unsigned char comp_smem[];
   LabelScalars *sc = a.sc;
