@@ -73,6 +73,8 @@ def parse():
                     help="length of the plain per-frame replay of the same streams")
     ap.add_argument("--no-4m", action="store_true")
     ap.add_argument("--no-u32", action="store_true")
+    ap.add_argument("--no-stills", action="store_true")
+    ap.add_argument("--serve-child", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the check of one step's output against the oracle")
     ap.add_argument("--no-tune", action="store_true",
@@ -514,9 +516,13 @@ def run_ours(args, ranks):
     if ranks.rank == 0 and not args.no_u32:
         u32 = u32_16m(args.steps)
 
+    stills = None
+    if ranks.rank == 0 and not args.no_stills:
+        stills = stills_uneven()
+
     served = None
     if ranks.rank == 0 and args.serve_seconds > 0:
-        served = serving(args.serve_seconds, args.plain_seconds, pool)
+        served = serving_process(args.serve_seconds, args.plain_seconds)
 
     cpu = None
     if ranks.rank == 0 and ranks.world == 1 and not args.no_cpu:
@@ -532,7 +538,7 @@ def run_ours(args, ranks):
     # keep_table, flatten, mark, compact, count, rank, scatter, accept (small
     # and large components), write, carry, finalize, and 5 scans of 3
     # launches
-    launches_per_step = 1 + 3 + (15 + 5 * 3)
+    launches_per_step = 1 + 3 + (16 + 5 * 3)
     # the whole pipeline's algorithmic bytes per frame: one read of the
     # frame, the signal list written and read back by the grouping, the
     # spot rows written
@@ -578,6 +584,7 @@ def run_ours(args, ranks):
         "reference_gpu": ref_gpu,
         "batched_vs_plain_4m": four_m,
         "u32_16m": u32,
+        "stills_uneven": stills,
         "latency": ({"frame_to_mask_p99_ms": {
                         name: r["frame_to_mask_ms"]["p99"]
                         for name, r in zip(("4m_500hz", "16m_100hz"), served["served"])},
@@ -737,6 +744,47 @@ def batched_vs_plain_4m(steps: int = 12):
     return out
 
 
+def stills_uneven(frames_per_series: int = 500):
+    """Uneven batched stills: four series of panel sizes 1028x1062,
+    2068x2162, 3110x3269 and 4148x4362 (fast x slow) interleaved in the same
+    launches, four frames of each per launch, 2D grouping (each frame on its
+    own), frames resident, CUDA events; `frames_per_series` frames of each
+    series in all. Spot density 0.5 per 1000 px^2 as the stills
+    configuration has it."""
+    from dials_metal_spotfinder_b200.engine import Engine
+    synth = load_synth()
+    per = 4
+    shapes = [tuple(s) for s in synth.STILL_SHAPES]
+    pools = [[synth.still(s, frames=8).frame(f) for f in range(8)] for s in shapes]
+    layout = [k for k in range(len(shapes)) for _ in range(per)]
+    steps = max(1, frames_per_series // per)
+    with Engine([shapes[k] for k in layout], np.uint16, slots=2) as eng:
+        eng.enable_grouping(first_frame=0, two_d=True)
+        for s in range(2):
+            for f, k in enumerate(layout):
+                eng.upload(s, f, pools[k][(s * per + f % per) % 8])
+        eng.synchronize()
+        for i in range(3):
+            eng.run(i % 2)
+        eng.synchronize()
+        eng.record(0)
+        for i in range(steps):
+            eng.run(i % 2)
+        eng.record(1)
+        eng.synchronize()
+        ms = eng.elapsed_ms(0, 1)
+        spots = sum(eng.group_counts(k)[0]["accepted"] for k in range(eng.nseries()))
+    frames = steps * len(layout)
+    px = steps * per * sum(h * w for h, w in shapes)
+    return {"workload": "uneven stills: 1028x1062, 2068x2162, 3110x3269, 4148x4362 uint16, "
+                        "interleaved, 2D grouping", "unit": UNIT,
+            "value": frames / (ms / 1e3), "frames_per_step": len(layout),
+            "frames_per_series": steps * per, "gpixels_per_s": px / (ms / 1e3) / 1e9,
+            "ms_per_step": ms / steps, "spots": spots,
+            "form": "batched engine, resident frames (8 distinct per series, cycled), "
+                    "CUDA events"}
+
+
 def u32_16m(steps: int):
     """The 16M uint32 variant (intensities up to 2e6): threshold + 3D
     grouping through the batched engine, frames resident, CUDA events as the
@@ -813,6 +861,27 @@ def serving(seconds: float, plain_seconds: float, pool16):
     return out
 
 
+def serving_process(seconds: float, plain_seconds: float):
+    """`serving` in a Python process of its own, as a detector's server runs:
+    this process has by then held several engines, gigabytes of page-locked
+    buffers and thread pools, none of which a server shares a process with.
+    The child makes the same 16M frames from the same seeds."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--serve-child",
+           "--serve-seconds", str(seconds), "--plain-seconds", str(plain_seconds)]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True,
+                           timeout=seconds + plain_seconds + 900)
+    except subprocess.TimeoutExpired:
+        return {"error": "the serving process did not finish"}
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    if r.returncode != 0 or not lines:
+        tail = (r.stderr.strip().splitlines() or ["no output"])[-1]
+        return {"error": f"the serving process exited {r.returncode}: {tail}"}
+    out = json.loads(lines[-1])
+    out["process"] = "a process of its own"
+    return out
+
+
 def reference_gpu_form(frame):
     """The reference's own CUDA backend (src/dext_cuda.cu via its gpu::find),
     built for sm_100a from the reference sources, on the same frame."""
@@ -846,6 +915,10 @@ def reference_gpu_form(frame):
 
 def main():
     args = parse()
+    if args.serve_child:
+        print(json.dumps(serving(args.serve_seconds, args.plain_seconds, make_pool(24))),
+              flush=True)
+        return
     ranks = Ranks()
     try:
         if args.impl == "reference":

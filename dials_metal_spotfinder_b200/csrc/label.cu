@@ -51,13 +51,41 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr uint32_t kNone = 0xffffffffu;
 constexpr int kThreads = 256;
-// Components up to this many members take lab_accept's launch with small
-// per-warp buffers (many warps per SM); the few larger ones are listed by
-// lab_rank and taken by a second launch with large buffers.
+// Components up to kSmallCap members take lab_accept's launch with small
+// per-warp buffers (many warps per SM); the larger ones are listed by
+// lab_rank in two lists, up to kMidCap members and beyond, and taken by
+// launches with larger buffers.
 constexpr uint32_t kSmallCap = 256;
+constexpr uint32_t kMidCap = 512;
+
+// Quotients by one divisor fixed for a whole launch (the frame width), by a
+// multiply-high and two shifts: Granlund and Montgomery, "Division by
+// invariant integers using multiplication" (PLDI 1994), the form with a
+// 33-bit multiplier whose top bit is folded into an add. Exact for every
+// 32-bit dividend and divisor >= 1.
+struct DivU32 {
+  uint32_t d, m, s1, s2;
+  static DivU32 of(uint32_t d) {
+    uint32_t l = 0;
+    while (l < 32 && (1ull << l) < d)
+      l++; // ceil(log2 d)
+    DivU32 v;
+    v.d = d;
+    v.m = static_cast<uint32_t>((((1ull << l) - d) << 32) / d + 1);
+    v.s1 = l < 1 ? l : 1;
+    v.s2 = l > 1 ? l - 1 : 0;
+    return v;
+  }
+  __device__ __forceinline__ uint32_t quo(uint32_t n) const {
+    const uint32_t t = __umulhi(m, n);
+    return (t + ((n - t) >> s1)) >> s2;
+  }
+  __device__ __forceinline__ uint32_t rem(uint32_t n) const { return n - quo(n) * d; }
+};
 
 struct LabArgs {
   int32_t width;
+  DivU32 wdiv; // division by the width
   int32_t nframes;
   int32_t close_all;
   int32_t two_d;
@@ -86,7 +114,8 @@ struct LabArgs {
   Pixel *pix_tmp;
   uint64_t *pack;
   uint32_t *obits, *ocnt; // open pixels: bitmap and (scanned) count per 32 positions
-  uint32_t *big; // ranks of the kept components with more than kSmallCap members
+  uint32_t *big; // ranks of the kept components with more than kMidCap members
+  uint32_t *mid; // ... with more than kSmallCap and at most kMidCap
   Spot *spots;
   Pixel *kept;
   uint64_t *seg_start, *seg_count;
@@ -229,7 +258,8 @@ __global__ void lab_setup(LabArgs a) {
   sc->closed32 = sc->open32 = 0;
   sc->runs_n = 0;
   sc->big_n = 0;
-  sc->link_next = sc->accept_next = sc->big_next = 0;
+  sc->mid_n = 0;
+  sc->link_next = sc->accept_next = sc->big_next = sc->mid_next = 0;
   sc->members_pack = 0;
   sc->accepted_pack = 0;
 }
@@ -259,7 +289,6 @@ __global__ void __launch_bounds__(kThreads) lab_gather(LabArgs a) {
   const uint64_t n = sc->n, carry = sc->carry_n;
   const int nseg = static_cast<int>(sc->nseg);
   const int first_batch_seg = carry > 0 ? 1 : 0;
-  const uint32_t W = static_cast<uint32_t>(a.width);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   __shared__ uint32_t warp_count[kThreads / 32];
   __shared__ uint32_t block_at;
@@ -300,7 +329,7 @@ __global__ void __launch_bounds__(kThreads) lab_gather(LabArgs a) {
         a.val[g] = px.value;
         pidx = px.index;
         const uint32_t prev = i == 0 ? 0u : list[i - 1].index;
-        left = i > 0 && px.index % W != 0 && prev + 1 == px.index;
+        left = i > 0 && prev + 1 == px.index && a.wdiv.rem(px.index) != 0;
         // This pixel is the first of every block from the one after the
         // previous pixel's up to its own.
         uint32_t *tab = a.tab + static_cast<uint64_t>(f) * a.nblk;
@@ -311,7 +340,7 @@ __global__ void __launch_bounds__(kThreads) lab_gather(LabArgs a) {
       } else if (g > sc->carry_last_start) {
         // the carried last frame, which the first batch frame links to
         const uint32_t v = a.ix[g];
-        left = v % W != 0 && a.ix[g - 1] + 1 == v;
+        left = a.ix[g - 1] + 1 == v && a.wdiv.rem(v) != 0;
       }
     }
     const uint32_t linked = __ballot_sync(kFull, left);
@@ -593,8 +622,10 @@ __global__ void __launch_bounds__(kThreads) lab_rank(LabArgs a) {
     const bool keep = size >= a.min_size && size <= a.max_size;
     a.msize[rank] = keep ? size : 0u;
     a.mpk[rank] = keep ? (static_cast<uint64_t>(size) | (1ull << 32)) : 0ull;
-    if (keep && size > kSmallCap)
+    if (keep && size > kMidCap)
       a.big[atomicAdd(&sc->big_n, 1u)] = rank;
+    else if (keep && size > kSmallCap)
+      a.mid[atomicAdd(&sc->mid_n, 1u)] = rank;
     small += size < a.min_size;
     large += size > a.max_size;
   }
@@ -689,7 +720,7 @@ struct SharedMembers {
 // nothing is fused). Returns whether the spot passes the peak-centroid
 // filter; fills *spot either way.
 template <typename Members>
-__device__ bool spot_pass(uint32_t W, double max_sep, const Members &mem, uint32_t n,
+__device__ bool spot_pass(const DivU32 &W, double max_sep, const Members &mem, uint32_t n,
                           Spot *spot) {
   const double pixel_variance = 1.0 / 12.0;
   double sum = 0.0, sum_sq = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
@@ -700,8 +731,9 @@ __device__ bool spot_pass(uint32_t W, double max_sep, const Members &mem, uint32
     uint32_t idx, v;
     int32_t z;
     mem.get(k, &idx, &v, &z);
-    const int32_t x = static_cast<int32_t>(idx % W);
-    const int32_t y = static_cast<int32_t>(idx / W);
+    const uint32_t yq = W.quo(idx);
+    const int32_t x = static_cast<int32_t>(idx - yq * W.d);
+    const int32_t y = static_cast<int32_t>(yq);
     if (k == 0) {
       x0 = x; x1 = x + 1; y0 = y; y1 = y + 1; z0 = z; z1 = z + 1;
     } else {
@@ -738,8 +770,9 @@ __device__ bool spot_pass(uint32_t W, double max_sep, const Members &mem, uint32
       int32_t z;
       mem.get(k, &idx, &v, &z);
       const double value = __uint2double_rn(v);
-      const double dx = __dsub_rn(__dadd_rn(__uint2double_rn(idx % W), 0.5), mx);
-      const double dy = __dsub_rn(__dadd_rn(__uint2double_rn(idx / W), 0.5), my);
+      const uint32_t yq = W.quo(idx);
+      const double dx = __dsub_rn(__dadd_rn(__uint2double_rn(idx - yq * W.d), 0.5), mx);
+      const double dy = __dsub_rn(__dadd_rn(__uint2double_rn(yq), 0.5), my);
       const double dz = __dsub_rn(__dadd_rn(__int2double_rn(z), 0.5), mz);
       dx2 = __dadd_rn(dx2, __dmul_rn(__dmul_rn(value, dx), dx));
       dy2 = __dadd_rn(dy2, __dmul_rn(__dmul_rn(value, dy), dy));
@@ -793,9 +826,10 @@ struct WarpBuffers {
   double *t; // 3 x 32 second-pass terms
 };
 
-// Per warp: four CAP-member arrays and the terms. Two launches split the
+// Per warp: four CAP-member arrays and the terms. Three launches split the
 // components by size: up to kSmallCap members with small buffers, so that
-// many warps fit on an SM, and the rest with kCompCap-member buffers.
+// many warps fit on an SM, up to kMidCap with middle ones, and the rest with
+// kCompCap-member buffers.
 
 template <uint32_t CAP> __host__ __device__ constexpr size_t warp_comp_bytes() {
   return 4 * CAP * sizeof(uint32_t) + 3 * 32 * sizeof(double);
@@ -970,8 +1004,8 @@ __device__ __forceinline__ int32_t warp_max(int32_t v) {
 // parallel but added in member order, one after another, as the reference
 // adds them. Returns false (and leaves *spot alone) if the first pass is not
 // exact for this component; *ok is the peak-centroid filter's verdict.
-__device__ bool spot_pass_warp(uint32_t W, double max_sep, const WarpBuffers &b, uint32_t n,
-                               int lane, Spot *spot, bool *ok) {
+__device__ bool spot_pass_warp(const DivU32 &W, double max_sep, const WarpBuffers &b,
+                               uint32_t n, int lane, Spot *spot, bool *ok) {
   double sum = 0.0, sum_sq = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
   int32_t x0 = INT_MAX, x1 = INT_MIN, y0 = INT_MAX, y1 = INT_MIN, z0 = INT_MAX, z1 = INT_MIN;
   uint32_t peak_v = 0, peak_k = kNone, max_v = 0;
@@ -979,7 +1013,8 @@ __device__ bool spot_pass_warp(uint32_t W, double max_sep, const WarpBuffers &b,
   for (uint32_t k = lane; k < n; k += 32) {
     const uint32_t idx = b.ix[k], v = b.val[k];
     const int32_t z = b.fr[k];
-    const int32_t x = static_cast<int32_t>(idx % W), y = static_cast<int32_t>(idx / W);
+    const uint32_t yq = W.quo(idx);
+    const int32_t x = static_cast<int32_t>(idx - yq * W.d), y = static_cast<int32_t>(yq);
     const double value = __uint2double_rn(v);
     sum = __dadd_rn(sum, value);
     sum_sq = __dadd_rn(sum_sq, __dmul_rn(value, value));
@@ -1024,8 +1059,9 @@ __device__ bool spot_pass_warp(uint32_t W, double max_sep, const WarpBuffers &b,
     pk = min(pk, __shfl_xor_sync(kFull, pk, d));
   double px = 0.0, py = 0.0, pz = 0.0;
   if (max_v > 0 && pk != kNone) {
-    px = __dadd_rn(__uint2double_rn(b.ix[pk] % W), 0.5);
-    py = __dadd_rn(__uint2double_rn(b.ix[pk] / W), 0.5);
+    const uint32_t pidx = b.ix[pk], pq = W.quo(pidx);
+    px = __dadd_rn(__uint2double_rn(pidx - pq * W.d), 0.5);
+    py = __dadd_rn(__uint2double_rn(pq), 0.5);
     pz = __dadd_rn(__int2double_rn(b.fr[pk]), 0.5);
   }
 
@@ -1040,26 +1076,35 @@ __device__ bool spot_pass_warp(uint32_t W, double max_sep, const WarpBuffers &b,
     const double mx = __ddiv_rn(wx, sum), my = __ddiv_rn(wy, sum);
     double mz = __ddiv_rn(wz, sum);
     // lanes 0, 1 and 2 each run one of the three sums, over terms the
-    // whole warp computes 32 at a time
+    // whole warp computes 32 at a time. Every term value * d * d is +0 or
+    // positive (value >= 0, and the two factors d have one sign), so the
+    // sums are too, and the +0 terms past the last member leave them
+    // unchanged: each chunk is 32 additions with no bound to test.
     double acc = 0.0;
     for (uint32_t c = 0; c < n; c += 32) {
       const uint32_t k = c + lane;
+      double tx = 0.0, ty = 0.0, tz = 0.0;
       if (k < n) {
-        const uint32_t idx = b.ix[k];
+        const uint32_t idx = b.ix[k], yq = W.quo(idx);
         const double value = __uint2double_rn(b.val[k]);
-        const double dx = __dsub_rn(__dadd_rn(__uint2double_rn(idx % W), 0.5), mx);
-        const double dy = __dsub_rn(__dadd_rn(__uint2double_rn(idx / W), 0.5), my);
+        const double dx = __dsub_rn(__dadd_rn(__uint2double_rn(idx - yq * W.d), 0.5), mx);
+        const double dy = __dsub_rn(__dadd_rn(__uint2double_rn(yq), 0.5), my);
         const double dz = __dsub_rn(__dadd_rn(__int2double_rn(b.fr[k]), 0.5), mz);
-        b.t[lane] = __dmul_rn(__dmul_rn(value, dx), dx);
-        b.t[32 + lane] = __dmul_rn(__dmul_rn(value, dy), dy);
-        b.t[64 + lane] = __dmul_rn(__dmul_rn(value, dz), dz);
+        tx = __dmul_rn(__dmul_rn(value, dx), dx);
+        ty = __dmul_rn(__dmul_rn(value, dy), dy);
+        tz = __dmul_rn(__dmul_rn(value, dz), dz);
       }
+      b.t[lane] = tx;
+      b.t[32 + lane] = ty;
+      b.t[64 + lane] = tz;
       __syncwarp();
       if (lane < 3) {
-        const uint32_t cnt = min(32u, n - c);
-        const double *t = b.t + 32 * lane;
-        for (uint32_t j = 0; j < cnt; j++)
-          acc = __dadd_rn(acc, t[j]);
+        const double2 *t = reinterpret_cast<const double2 *>(b.t + 32 * lane);
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+          const double2 u = t[j];
+          acc = __dadd_rn(__dadd_rn(acc, u.x), u.y);
+        }
       }
       __syncwarp();
     }
@@ -1105,18 +1150,22 @@ __device__ bool spot_pass_warp(uint32_t W, double max_sep, const WarpBuffers &b,
 // where the accepted ones go.
 // Components of lo < size <= hi; the launch with lo = 0 also clears the
 // pack word of those the size filter removed.
-// With `listed`, the components are lab_rank's list of the large ones
-// rather than every finished root.
+// `list` says which components a launch walks: 0 every finished root, 1
+// lab_rank's list of the large ones, 2 its list of the middle-sized ones.
+// Blocks per SM for a buffer size: as many as its shared memory allows.
+template <uint32_t CAP> constexpr int kAcceptBlocks = CAP <= 256 ? 8 : CAP <= 512 ? 6 : 1;
+
 template <uint32_t CAP>
-__global__ void __launch_bounds__(kCompWarps * 32, CAP <= 256 ? 8 : 1) lab_accept(LabArgs a, uint32_t lo,
-                                                              uint32_t hi, int listed) {
+__global__ void __launch_bounds__(kCompWarps * 32, kAcceptBlocks<CAP>)
+    lab_accept(LabArgs a, uint32_t lo, uint32_t hi, int list) {
   extern __shared__ __align__(16) unsigned char comp_smem[];
   LabelScalars *sc = a.sc;
-  const uint64_t closed = listed ? sc->big_n : sc->closed;
-  uint32_t *next = listed ? &sc->big_next : &sc->accept_next;
+  const uint64_t closed = list == 0 ? sc->closed : list == 1 ? sc->big_n : sc->mid_n;
+  uint32_t *next = list == 0 ? &sc->accept_next : list == 1 ? &sc->big_next : &sc->mid_next;
+  const uint32_t *listed = list == 1 ? a.big : a.mid;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const WarpBuffers b = warp_buffers<CAP>(comp_smem, warp);
-  const uint32_t W = static_cast<uint32_t>(a.width);
+  const DivU32 W = a.wdiv;
   uint32_t separated = 0;
   // a warp takes the next component when it has finished its last
   while (true) {
@@ -1126,7 +1175,7 @@ __global__ void __launch_bounds__(kCompWarps * 32, CAP <= 256 ? 8 : 1) lab_accep
     i = __shfl_sync(kFull, i, 0);
     if (i >= closed)
       break;
-    const uint64_t r = listed ? a.big[i] : i;
+    const uint64_t r = list == 0 ? i : listed[i];
     const uint32_t n = a.msize[r];
     if (n == 0) {
       if (lane == 0 && lo == 0)
@@ -1320,13 +1369,13 @@ void DeviceLabeller::release() {
   }
   void *ptrs[] = {root_, size_, rank_of_root_, cursor_, lastz_, bits_, bcnt_, flist_, comp_root_,
                   msize_, mpk_, runs_, run_starts_, spot_tmp_, pix_tmp_, members_, pack_, obits_, ocnt_, spots_out_, kept_out_, seg_start_,
-                  seg_count_, seg_z_, tab_, big_};
+                  seg_count_, seg_z_, tab_, big_, mid_};
   for (void *p : ptrs)
     cudaFree(p);
   tab_ = nullptr;
   root_ = size_ = rank_of_root_ = cursor_ = nullptr;
   lastz_ = nullptr;
-  bits_ = bcnt_ = flist_ = comp_root_ = msize_ = members_ = obits_ = ocnt_ = big_ = nullptr;
+  bits_ = bcnt_ = flist_ = comp_root_ = msize_ = members_ = obits_ = ocnt_ = big_ = mid_ = nullptr;
   mpk_ = pack_ = nullptr;
   runs_ = nullptr;
   run_starts_ = nullptr;
@@ -1391,7 +1440,8 @@ void DeviceLabeller::reserve(uint64_t batch_pixels, int max_frames, uint64_t car
     alloc(&pack_, live, "spot offsets");
     alloc(&obits_, nwmax, "open bitmap");
     alloc(&ocnt_, nwmax, "open counts");
-    alloc(&big_, live / (kSmallCap + 1) + 1, "large components");
+    alloc(&big_, live / (kMidCap + 1) + 1, "large components");
+    alloc(&mid_, live / (kSmallCap + 1) + 1, "middle-sized components");
     alloc(&spots_out_, spot_cap, "spots");
     alloc(&spot_tmp_, spot_cap, "spot scratch");
     alloc(&pix_tmp_, live, "spot pixel scratch");
@@ -1440,6 +1490,7 @@ void DeviceLabeller::enqueue(int nframes, const SignalPixel *lists, const uint64
     throw std::invalid_argument("the labeller has no capacity: reserve() first");
   LabArgs a;
   a.width = width_;
+  a.wdiv = DivU32::of(static_cast<uint32_t>(width_));
   a.nframes = nframes;
   a.close_all = close_all ? 1 : 0;
   a.two_d = opt_.two_d ? 1 : 0;
@@ -1483,6 +1534,7 @@ void DeviceLabeller::enqueue(int nframes, const SignalPixel *lists, const uint64
   a.obits = obits_;
   a.ocnt = ocnt_;
   a.big = big_;
+  a.mid = mid_;
   a.spots = spots_out_;
   a.kept = kept_out_;
   a.seg_start = seg_start_;
@@ -1517,9 +1569,11 @@ void DeviceLabeller::enqueue(int nframes, const SignalPixel *lists, const uint64
   check(cudaEventRecord(fork_, s), "cudaEventRecord");
   check(cudaStreamWaitEvent(aux_, fork_, 0), "cudaStreamWaitEvent");
   lab_accept<kCompCap><<<grid_ / 4, kCompWarps * 32, kCompWarps * warp_comp_bytes<kCompCap>(),
-                         aux_>>>(a, kSmallCap, 0xffffffffu, 1);
+                         aux_>>>(a, kMidCap, 0xffffffffu, 1);
   lab_accept<kSmallCap><<<grid, kCompWarps * 32, kCompWarps * warp_comp_bytes<kSmallCap>(), s>>>(
       a, 0u, kSmallCap, 0);
+  lab_accept<kMidCap><<<grid_ / 8 * kAcceptBlocks<kMidCap>, kCompWarps * 32,
+                        kCompWarps * warp_comp_bytes<kMidCap>(), s>>>(a, kSmallCap, kMidCap, 2);
   check(cudaEventRecord(join_, aux_), "cudaEventRecord");
   check(cudaStreamWaitEvent(s, join_, 0), "cudaStreamWaitEvent");
   scan64_.run(pack_, pack_, &sc->closed, 1, live_cap_, &sc->accepted_pack, s);

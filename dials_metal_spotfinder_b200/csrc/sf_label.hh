@@ -51,11 +51,13 @@ struct LabelScalars {
   uint64_t closed;        // finished components
   uint32_t closed32, open32;
   uint32_t runs_n;        // lab_link's work list
-  uint32_t big_n;         // components past the small spot-pass buffers
+  uint32_t big_n;         // components past the middle spot-pass buffers
   // work counters: warps take the next entries as they finish their last,
   // so a few long union-find chains or large components do not hold a
   // whole grid-stride share
-  uint32_t link_next, accept_next, big_next, pad0;
+  uint32_t link_next, accept_next, big_next, mid_next;
+  uint32_t mid_n;         // components past the small buffers, within the middle ones
+  uint32_t pad0;
   uint64_t members_pack;  // members (low 32) | components passing the size filters (high 32)
   uint64_t accepted_pack; // accepted spots (low 32) | their pixels (high 32)
   uint64_t batch_spots, batch_pixels;
@@ -144,6 +146,7 @@ private:
   uint64_t *pack_ = nullptr;
   uint32_t *obits_ = nullptr, *ocnt_ = nullptr; // open pixels per 32 positions
   uint32_t *big_ = nullptr; // ranks of the components lab_accept's large launch takes
+  uint32_t *mid_ = nullptr; // ... and its middle launch
   Spot *spots_out_ = nullptr;
   Pixel *kept_out_ = nullptr;
   uint64_t *seg_start_ = nullptr; // per batch segment: start, count (device)

@@ -111,7 +111,7 @@ def test_bench_line_has_the_contract_keys(monkeypatch):
                         lambda n: [np.zeros(bench.SHAPE, np.uint16) for _ in range(n)])
     monkeypatch.setattr(sys, "argv", ["bench.py", "--steps", "2", "--warmup", "3", "--no-cpu",
                                       "--serve-seconds", "0", "--no-4m", "--e2e-steps", "2",
-                                      "--pool", "2", "--no-tune", "--no-u32"])
+                                      "--pool", "2", "--no-tune", "--no-u32", "--no-stills"])
     out = io.StringIO()
     with contextlib.redirect_stdout(out):
         bench.main()
