@@ -883,6 +883,8 @@ __device__ __forceinline__ bool run_start(const uint32_t *g, uint32_t k, uint32_
 // runs: their chunks are sorted (the chunks of one component are distinct),
 // each run finds its rank by binary search, and every member moves once.
 // Uses b.ix, b.val and b.fr as scratch.
+__device__ void move_runs(const WarpBuffers &b, uint32_t n, int lane);
+
 __device__ void order_members(const WarpBuffers &b, uint32_t n, int lane) {
   const uint32_t lt = (1u << lane) - 1u;
   uint32_t runs = 0;
@@ -897,6 +899,42 @@ __device__ void order_members(const WarpBuffers &b, uint32_t n, int lane) {
   __syncwarp();
   if (runs == 1)
     return; // one chunk: already ascending
+  if (runs <= 32) {
+    // One run per lane. Sort the keys chunk << 5 | run (chunks are below
+    // 2^27) across the lanes with a bitonic network in registers; lane q then
+    // holds the run of rank q, whose place is the sum of the lengths of the
+    // runs ranked before it.
+    const bool have = static_cast<uint32_t>(lane) < runs;
+    const uint32_t s0 = have ? b.ix[lane] : 0u;
+    const uint32_t s1 = static_cast<uint32_t>(lane) + 1 < runs ? b.ix[lane + 1] : n;
+    const uint32_t len = have ? s1 - s0 : 0u;
+    uint32_t key = have ? (b.g[s0] & ~31u) | static_cast<uint32_t>(lane) : 0xffffffffu;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        const uint32_t other = __shfl_xor_sync(kFull, key, j);
+        const bool ascending = (lane & k) == 0, lower = (lane & j) == 0;
+        key = lower == ascending ? min(key, other) : max(key, other);
+      }
+    }
+    const int run = static_cast<int>(key & 31u); // valid on lanes below runs
+    const uint32_t rlen = __shfl_sync(kFull, len, run);
+    const uint32_t rs0 = __shfl_sync(kFull, s0, run);
+    uint32_t incl = have ? rlen : 0u;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t v = __shfl_up_sync(kFull, incl, d);
+      if (lane >= d)
+        incl += v;
+    }
+    __syncwarp(); // every lane has read its start before any is overwritten
+    if (have)
+      b.ix[run] = rs0 | ((incl - rlen) << 16); // start and place, both below kCompCap
+    __syncwarp();
+    move_runs(b, n, lane);
+    return;
+  }
   for (uint32_t j = lane; j < runs; j += 32)
     b.val[j] = b.g[b.ix[j]] >> 5;
   __syncwarp();
@@ -940,6 +978,13 @@ __device__ void order_members(const WarpBuffers &b, uint32_t n, int lane) {
     b.ix[j] = s0 | (off << 16); // start and place, both below kCompCap
   }
   __syncwarp();
+  move_runs(b, n, lane);
+}
+
+// Moves every member to its run's place plus its offset in the run (b.ix
+// holds start | place << 16 per run, in run order) through b.fr.
+__device__ void move_runs(const WarpBuffers &b, uint32_t n, int lane) {
+  const uint32_t lt = (1u << lane) - 1u;
   uint32_t base = 0;
   for (uint32_t c = 0; c < n; c += 32) {
     const uint32_t k = c + lane;
