@@ -113,6 +113,32 @@ struct Pending {
   int64_t t_submit;
 };
 
+// Latency samples, appended in fixed blocks: an append never moves the
+// samples already stored. (A vector that doubles copies all of them, and a
+// series' spot samples reach tens of millions within a minute -- a copy of
+// hundreds of megabytes made while the series' lock is held, which stalls
+// every submission meanwhile.)
+class Samples {
+public:
+  void push_back(double v) {
+    if (n_ == blocks_.size() * kBlock)
+      blocks_.emplace_back(new double[kBlock]);
+    blocks_[n_ / kBlock][n_ % kBlock] = v;
+    n_++;
+  }
+  size_t size() const { return n_; }
+  void copy_to(double *out) const {
+    for (size_t b = 0; b * kBlock < n_; b++)
+      std::memcpy(out + b * kBlock, blocks_[b].get(),
+                  std::min(kBlock, n_ - b * kBlock) * sizeof(double));
+  }
+
+private:
+  static constexpr size_t kBlock = size_t(1) << 16;
+  std::vector<std::unique_ptr<double[]>> blocks_;
+  size_t n_ = 0;
+};
+
 struct ServerSeries {
   int id = 0;
   int device = 0;
@@ -142,7 +168,7 @@ struct ServerSeries {
   std::vector<uint32_t> signal_counts;
   std::vector<int64_t> t_submit; // per frame number
   int64_t t_close = 0;           // when the series was closed
-  std::vector<double> lat_mask, lat_grouped, lat_spot;
+  Samples lat_mask, lat_grouped, lat_spot;
   sf_counts counts{};
   uint64_t frames_done = 0, dropped = 0;
   std::string error;
@@ -494,6 +520,14 @@ using sf::ServerSeries;
 
 namespace {
 
+int copy_out(const sf::Samples &v, double *out, size_t capacity, size_t *n) {
+  *n = v.size();
+  if (v.size() > capacity)
+    return -2;
+  v.copy_to(out);
+  return 0;
+}
+
 template <typename T>
 int copy_out(const std::vector<T> &v, T *out, size_t capacity, size_t *n) {
   *n = v.size();
@@ -697,8 +731,7 @@ int sf_server_latencies(sf_server *server, int series, int kind, double *out, si
       return -1;
     ServerSeries &se = reinterpret_cast<Server *>(server)->at(series);
     std::lock_guard<std::mutex> g(se.m);
-    const std::vector<double> &v =
-        kind == 0 ? se.lat_mask : kind == 1 ? se.lat_grouped : se.lat_spot;
+    const sf::Samples &v = kind == 0 ? se.lat_mask : kind == 1 ? se.lat_grouped : se.lat_spot;
     return copy_out(v, out, capacity, n);
   });
 }
