@@ -1383,12 +1383,20 @@ DeviceLabeller::DeviceLabeller(int height, int width, const GroupOptions &option
   grid_ = static_cast<unsigned>(device_sm_count() * 8);
   check(cudaMallocHost(&z_stage_, sizeof(int64_t)), "cudaMallocHost");
   check(cudaStreamCreateWithFlags(&aux_, cudaStreamNonBlocking), "cudaStreamCreate");
+  check(cudaStreamCreateWithFlags(&aux2_, cudaStreamNonBlocking), "cudaStreamCreate");
   check(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "cudaEventCreate");
   check(cudaEventCreateWithFlags(&join_, cudaEventDisableTiming), "cudaEventCreate");
+  check(cudaEventCreateWithFlags(&join2_, cudaEventDisableTiming), "cudaEventCreate");
   check(cudaStreamSynchronize(cudaStreamLegacy), "clearing labeller scalars");
 }
 
 DeviceLabeller::~DeviceLabeller() {
+  if (aux2_) {
+    cudaStreamSynchronize(aux2_);
+    cudaStreamDestroy(aux2_);
+  }
+  if (join2_)
+    cudaEventDestroy(join2_);
   if (aux_) {
     cudaStreamSynchronize(aux_);
     cudaStreamDestroy(aux_);
@@ -1610,17 +1618,23 @@ void DeviceLabeller::enqueue(int nframes, const SignalPixel *lists, const uint64
   lab_rank<<<grid, kThreads, 0, s>>>(a);
   scan64_.run(mpk_, mpk_, &sc->closed, 1, live_cap_, &sc->members_pack, s);
   lab_scatter<<<grid, kThreads, 0, s>>>(a);
-  // the few large components on a second stream, beside the many small
+  // The few large and middle-sized components on streams of their own,
+  // launched first so that their blocks are placed before the many small
+  // components' launch fills the SMs: each of them is one warp's long walk,
+  // which then runs beside the small ones instead of after them.
   check(cudaEventRecord(fork_, s), "cudaEventRecord");
   check(cudaStreamWaitEvent(aux_, fork_, 0), "cudaStreamWaitEvent");
+  check(cudaStreamWaitEvent(aux2_, fork_, 0), "cudaStreamWaitEvent");
   lab_accept<kCompCap><<<grid_ / 4, kCompWarps * 32, kCompWarps * warp_comp_bytes<kCompCap>(),
                          aux_>>>(a, kMidCap, 0xffffffffu, 1);
+  lab_accept<kMidCap><<<grid_ / 8 * kAcceptBlocks<kMidCap>, kCompWarps * 32,
+                        kCompWarps * warp_comp_bytes<kMidCap>(), aux2_>>>(a, kSmallCap, kMidCap, 2);
   lab_accept<kSmallCap><<<grid, kCompWarps * 32, kCompWarps * warp_comp_bytes<kSmallCap>(), s>>>(
       a, 0u, kSmallCap, 0);
-  lab_accept<kMidCap><<<grid_ / 8 * kAcceptBlocks<kMidCap>, kCompWarps * 32,
-                        kCompWarps * warp_comp_bytes<kMidCap>(), s>>>(a, kSmallCap, kMidCap, 2);
   check(cudaEventRecord(join_, aux_), "cudaEventRecord");
+  check(cudaEventRecord(join2_, aux2_), "cudaEventRecord");
   check(cudaStreamWaitEvent(s, join_, 0), "cudaStreamWaitEvent");
+  check(cudaStreamWaitEvent(s, join2_, 0), "cudaStreamWaitEvent");
   scan64_.run(pack_, pack_, &sc->closed, 1, live_cap_, &sc->accepted_pack, s);
   lab_write<<<grid, kThreads, 0, s>>>(a);
   scan32_.run(ocnt_, ocnt_, &sc->nw, 1, nwmax, &sc->open32, s);

@@ -157,8 +157,9 @@ private:
   uint64_t nblk_ = 0;
   unsigned grid_ = 0;
   LabelScalars *sc_ = nullptr;
-  cudaStream_t aux_ = nullptr;                // the large components' spot pass
-  cudaEvent_t fork_ = nullptr, join_ = nullptr;
+  cudaStream_t aux_ = nullptr;  // the large components' spot pass
+  cudaStream_t aux2_ = nullptr; // the middle-sized components' spot pass
+  cudaEvent_t fork_ = nullptr, join_ = nullptr, join2_ = nullptr;
   int64_t *z_stage_ = nullptr; // pinned
 
   DeviceScan<uint32_t> scan32_;
