@@ -92,20 +92,24 @@ __global__ void __launch_bounds__(kPlaceThreads)
   const uint32_t grand = carry_s;
 
   // Each frame's first tile lies inside some block; its prefix is that
-  // block's prefix plus the counts in the block before it.
-  for (int f = 0; f < nframes; f++) {
+  // block's prefix plus the counts in the block before it. A warp per frame,
+  // so the frames' reads overlap.
+  const int lane = threadIdx.x & 31;
+  for (int f = threadIdx.x >> 5; f < nframes; f += kPlaceThreads / 32) {
     const uint64_t t0 = frames[f].tile_base;
     const uint64_t blk = t0 / kPlaceTiles;
     const uint64_t from = blk * kPlaceTiles;
     uint32_t part = 0;
-    for (uint64_t t = from + threadIdx.x; t < t0; t += kPlaceThreads)
+#pragma unroll 4
+    for (uint64_t t = from + lane; t < t0; t += 32)
       part += counts[t];
-    uint32_t total;
-    block_excl_scan(part, &total);
-    if (threadIdx.x == 0)
-      frame_prefix[f] = (blk < nblocks ? block_sums[blk] : grand) + total;
-    __syncthreads();
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1)
+      part += __shfl_xor_sync(kFull, part, d);
+    if (lane == 0)
+      frame_prefix[f] = (blk < nblocks ? block_sums[blk] : grand) + part;
   }
+  __syncthreads();
   if (threadIdx.x == 0)
     frame_prefix[nframes] = grand;
   __syncthreads();

@@ -2,10 +2,13 @@
 // memory, so that a pipeline of kernels can be enqueued (or captured in a
 // CUDA graph) without reading sizes back to the host. Three launches, no
 // inter-block waiting:
-//   scan_reduce  per-block sums of kScanTile elements
-//   scan_blocks  one block: exclusive scan of the block sums, and the total
-//   scan_down    per-block scan plus the block's prefix
-// Blocks past the device-side length return at once.
+//   scan_reduce  per-tile sums of kScanTile elements
+//   scan_blocks  one block: exclusive scan of the tile sums, and the total
+//   scan_down    per-tile scan plus the tile's prefix
+// The launches have one block per SM, which take the tiles up to the
+// device-side length in turn: a grid sized for the largest length the
+// caller allows would spend most of its time starting blocks that find
+// nothing to do (the lengths run far below their bounds).
 
 #include "sf_scan.cuh"
 
@@ -49,20 +52,21 @@ template <typename V>
 __global__ void __launch_bounds__(kScanThreads)
     scan_reduce(const V *in, const uint64_t *len, uint64_t len_scale, V *block_sums) {
   const uint64_t n = *len * len_scale;
-  const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kScanTile;
-  if (base >= n && blockIdx.x != 0)
-    return;
-  V sum = 0;
+  const uint64_t ntiles = n == 0 ? 1 : (n + kScanTile - 1) / kScanTile;
+  for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const uint64_t base = t * kScanTile;
+    V sum = 0;
 #pragma unroll
-  for (int i = 0; i < kScanItems; i++) {
-    const uint64_t at = base + static_cast<uint64_t>(i) * kScanThreads + threadIdx.x;
-    if (at < n)
-      sum += in[at];
+    for (int i = 0; i < kScanItems; i++) {
+      const uint64_t at = base + static_cast<uint64_t>(i) * kScanThreads + threadIdx.x;
+      if (at < n)
+        sum += in[at];
+    }
+    V total;
+    block_excl(sum, &total);
+    if (threadIdx.x == 0)
+      block_sums[t] = total;
   }
-  V total;
-  block_excl(sum, &total);
-  if (threadIdx.x == 0)
-    block_sums[blockIdx.x] = total;
 }
 
 template <typename V>
@@ -96,38 +100,39 @@ __global__ void __launch_bounds__(kScanThreads)
     scan_down(const V *in, const uint64_t *len, uint64_t len_scale, const V *block_sums,
               V *out) {
   const uint64_t n = *len * len_scale;
-  const uint64_t base = static_cast<uint64_t>(blockIdx.x) * kScanTile;
-  if (base >= n)
-    return;
   // Items are read strided (coalesced) and scanned per thread over a
   // transposed order: thread t owns items base + t*kScanItems + i.
   __shared__ V tile[kScanTile];
+  for (uint64_t t = blockIdx.x; t * kScanTile < n; t += gridDim.x) {
+    const uint64_t base = t * kScanTile;
 #pragma unroll
-  for (int i = 0; i < kScanItems; i++) {
-    const uint64_t at = base + static_cast<uint64_t>(i) * kScanThreads + threadIdx.x;
-    tile[i * kScanThreads + threadIdx.x] = at < n ? in[at] : V(0);
-  }
-  __syncthreads();
-  V run = 0;
-  V mine[kScanItems];
+    for (int i = 0; i < kScanItems; i++) {
+      const uint64_t at = base + static_cast<uint64_t>(i) * kScanThreads + threadIdx.x;
+      tile[i * kScanThreads + threadIdx.x] = at < n ? in[at] : V(0);
+    }
+    __syncthreads();
+    V run = 0;
+    V mine[kScanItems];
 #pragma unroll
-  for (int i = 0; i < kScanItems; i++) {
-    mine[i] = tile[threadIdx.x * kScanItems + i];
-    run += mine[i];
-  }
-  V total;
-  V pre = block_excl(run, &total) + block_sums[blockIdx.x];
+    for (int i = 0; i < kScanItems; i++) {
+      mine[i] = tile[threadIdx.x * kScanItems + i];
+      run += mine[i];
+    }
+    V total;
+    V pre = block_excl(run, &total) + block_sums[t];
 #pragma unroll
-  for (int i = 0; i < kScanItems; i++) {
-    tile[threadIdx.x * kScanItems + i] = pre;
-    pre += mine[i];
-  }
-  __syncthreads();
+    for (int i = 0; i < kScanItems; i++) {
+      tile[threadIdx.x * kScanItems + i] = pre;
+      pre += mine[i];
+    }
+    __syncthreads();
 #pragma unroll
-  for (int i = 0; i < kScanItems; i++) {
-    const uint64_t at = base + static_cast<uint64_t>(i) * kScanThreads + threadIdx.x;
-    if (at < n)
-      out[at] = tile[i * kScanThreads + threadIdx.x];
+    for (int i = 0; i < kScanItems; i++) {
+      const uint64_t at = base + static_cast<uint64_t>(i) * kScanThreads + threadIdx.x;
+      if (at < n)
+        out[at] = tile[i * kScanThreads + threadIdx.x];
+    }
+    __syncthreads(); // the tile is refilled by the next turn
   }
 }
 
@@ -143,6 +148,8 @@ void DeviceScan<V>::reserve(uint64_t max_len) {
   block_sums_ = nullptr;
   check(cudaMalloc(&block_sums_, blocks * sizeof(V)), "cudaMalloc scan workspace");
   max_blocks_ = blocks;
+  if (!grid_cap_)
+    grid_cap_ = static_cast<unsigned>(device_sm_count());
 }
 
 template <typename V> DeviceScan<V>::~DeviceScan() {
@@ -154,12 +161,11 @@ template <typename V>
 void DeviceScan<V>::run(const V *in, V *out, const uint64_t *len, uint64_t len_scale,
                         uint64_t max_len, V *total, cudaStream_t s) {
   reserve(max_len);
-  const uint64_t blocks = max_len / kScanTile + 1;
-  scan_reduce<V><<<static_cast<unsigned>(blocks), kScanThreads, 0, s>>>(in, len, len_scale,
-                                                                        block_sums_);
+  const unsigned grid =
+      static_cast<unsigned>(std::min<uint64_t>(max_len / kScanTile + 1, grid_cap_));
+  scan_reduce<V><<<grid, kScanThreads, 0, s>>>(in, len, len_scale, block_sums_);
   scan_blocks<V><<<1, kScanThreads, 0, s>>>(block_sums_, len, len_scale, total);
-  scan_down<V><<<static_cast<unsigned>(blocks), kScanThreads, 0, s>>>(in, len, len_scale,
-                                                                      block_sums_, out);
+  scan_down<V><<<grid, kScanThreads, 0, s>>>(in, len, len_scale, block_sums_, out);
   check(cudaGetLastError(), "launching a scan");
 }
 
