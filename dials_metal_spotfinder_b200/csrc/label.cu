@@ -461,8 +461,19 @@ __global__ void __launch_bounds__(kThreads) lab_link(LabArgs a) {
   const uint64_t *seg_count = in_shared ? sh_count : a.seg_count;
   const int64_t *seg_z = in_shared ? sh_z : a.seg_z;
   const int lane = threadIdx.x & 31;
-  // the links of entry i of lab_gather's list
-  auto link = [&](uint64_t i) {
+  // one entry of lab_gather's list per lane, so the lanes of a warp all
+  // have a run to link; a warp takes the next 32 entries when its last are
+  // done (chains vary in length, so fixed shares would leave warps idle)
+  while (true) {
+    uint32_t base = 0;
+    if (lane == 0)
+      base = atomicAdd(&sc->link_next, 32u);
+    base = __shfl_sync(kFull, base, 0);
+    if (base >= nruns)
+      break;
+    const uint64_t i = base + static_cast<uint64_t>(lane);
+    if (i >= nruns)
+      continue;
     const uint4 e = a.runs[i];
     const uint32_t g = e.x, idx = e.y;
     const uint32_t len = e.z & 0x3fu;
@@ -489,24 +500,6 @@ __global__ void __launch_bounds__(kThreads) lab_link(LabArgs a) {
       ra = unite_overlaps(a, ra, qu, s0, end - s0, last - W);
     if (prev)
       unite_overlaps(a, ra, qp, ps0, pcount, last);
-  };
-  // One entry per lane, so the lanes of a warp all have a run to link; a
-  // warp takes the next 32 entries when its last are done (chains vary in
-  // length, so fixed shares would leave warps idle). The next 32 are
-  // claimed when a batch starts, so that the claim's round trip to the
-  // counter overlaps the batch's links.
-  uint32_t base = 0;
-  if (lane == 0)
-    base = atomicAdd(&sc->link_next, 32u);
-  base = __shfl_sync(kFull, base, 0);
-  while (base < nruns) {
-    uint32_t claimed = 0;
-    if (lane == 0)
-      claimed = atomicAdd(&sc->link_next, 32u);
-    const uint64_t i = base + static_cast<uint64_t>(lane);
-    if (i < nruns)
-      link(i);
-    base = __shfl_sync(kFull, claimed, 0);
   }
 }
 
@@ -1205,7 +1198,7 @@ __device__ bool spot_pass_warp(const DivU32 &W, double max_sep, const WarpBuffer
 // `list` says which components a launch walks: 0 every finished root, 1
 // lab_rank's list of the large ones, 2 its list of the middle-sized ones.
 // Blocks per SM for a buffer size: as many as its shared memory allows.
-template <uint32_t CAP> constexpr int kAcceptBlocks = CAP <= 256 ? 7 : CAP <= 512 ? 6 : 1;
+template <uint32_t CAP> constexpr int kAcceptBlocks = CAP <= 256 ? 8 : CAP <= 512 ? 6 : 1;
 
 template <uint32_t CAP>
 __global__ void __launch_bounds__(kCompWarps * 32, kAcceptBlocks<CAP>)
@@ -1219,17 +1212,23 @@ __global__ void __launch_bounds__(kCompWarps * 32, kAcceptBlocks<CAP>)
   const WarpBuffers b = warp_buffers<CAP>(comp_smem, warp);
   const DivU32 W = a.wdiv;
   uint32_t separated = 0;
-  // component i of the launch's list
-  auto accept = [&](uint32_t i) {
+  // a warp takes the next component when it has finished its last
+  while (true) {
+    uint32_t i = 0;
+    if (lane == 0)
+      i = atomicAdd(next, 1u);
+    i = __shfl_sync(kFull, i, 0);
+    if (i >= closed)
+      break;
     const uint64_t r = list == 0 ? i : listed[i];
     const uint32_t n = a.msize[r];
     if (n == 0) {
       if (lane == 0 && lo == 0)
         a.pack[r] = 0;
-      return;
+      continue;
     }
     if (n <= lo || n > hi)
-      return;
+      continue;
     const uint32_t moff = static_cast<uint32_t>(a.mpk[r]);
     const uint32_t sidx = static_cast<uint32_t>(a.mpk[r] >> 32);
     uint32_t *m = a.members + moff;
@@ -1274,21 +1273,7 @@ __global__ void __launch_bounds__(kCompWarps * 32, kAcceptBlocks<CAP>)
         a.pack[r] = (static_cast<uint64_t>(n) << 32) | 1u;
       }
     }
-  };
-  // A warp takes the next component when it has finished its last; the
-  // next is claimed when one starts, so the claim's round trip to the
-  // counter overlaps the work.
-  uint32_t i = 0;
-  if (lane == 0)
-    i = atomicAdd(next, 1u);
-  i = __shfl_sync(kFull, i, 0);
-  while (i < closed) {
-    uint32_t claimed = 0;
-    if (lane == 0)
-      claimed = atomicAdd(next, 1u);
-    accept(i);
     __syncwarp();
-    i = __shfl_sync(kFull, claimed, 0);
   }
   if (lane == 0 && separated)
     atomicAdd(reinterpret_cast<unsigned long long *>(&sc->separated), separated);
@@ -1644,8 +1629,8 @@ void DeviceLabeller::enqueue(int nframes, const SignalPixel *lists, const uint64
                          aux_>>>(a, kMidCap, 0xffffffffu, 1);
   lab_accept<kMidCap><<<grid_ / 8 * kAcceptBlocks<kMidCap>, kCompWarps * 32,
                         kCompWarps * warp_comp_bytes<kMidCap>(), aux2_>>>(a, kSmallCap, kMidCap, 2);
-  lab_accept<kSmallCap><<<grid_ / 8 * kAcceptBlocks<kSmallCap>, kCompWarps * 32,
-                          kCompWarps * warp_comp_bytes<kSmallCap>(), s>>>(a, 0u, kSmallCap, 0);
+  lab_accept<kSmallCap><<<grid, kCompWarps * 32, kCompWarps * warp_comp_bytes<kSmallCap>(), s>>>(
+      a, 0u, kSmallCap, 0);
   check(cudaEventRecord(join_, aux_), "cudaEventRecord");
   check(cudaEventRecord(join2_, aux2_), "cudaEventRecord");
   check(cudaStreamWaitEvent(s, join_, 0), "cudaStreamWaitEvent");

@@ -277,6 +277,7 @@ struct Server {
     se->eng->post_run = post_run_sink;
     se->eng->post_arg = se.get();
     se->eng->use_graph = use_graph;
+    warm_up(*se);
     ServerSeries *raw = se.get();
     {
       std::lock_guard<std::mutex> g(m);
@@ -287,6 +288,36 @@ struct Server {
     raw->collector = std::thread([this, raw] { collect_loop(*raw); });
     *out = raw->id;
     return 0;
+  }
+
+  // Before a series takes frames: an empty frame, as a bitshuffle/LZ4
+  // chunk, through every slot and both of each slot's grouping graphs, so
+  // that the kernels are loaded and the graphs instantiated now and not
+  // while a detector streams its first frames (without this, two series
+  // opened together stalled for about half a second at their start and
+  // dropped frames); the labeller then expects the series' first frame. An
+  // empty frame has no signal pixels, so no count or result changes.
+  void warm_up(ServerSeries &se) {
+    Engine &e = *se.eng;
+    const ThresholdPlan::Shape sh = e.plan->shape(0);
+    const size_t n = static_cast<size_t>(sh.height) * sh.width;
+    const size_t eb = static_cast<size_t>(e.plan->elem_bytes());
+    std::vector<uint8_t> chunk;
+    {
+      std::vector<uint8_t> zeros(n * eb, 0);
+      encode_chunk(SF_CHUNK_BSLZ4, zeros.data(), n, eb, chunk);
+    }
+    if (chunk.size() > se.chunk_cap)
+      throw DeviceError("the empty frame's chunk exceeds the chunk bound");
+    std::memcpy(se.staging[0], chunk.data(), chunk.size());
+    const int slots = e.plan->nslots();
+    for (int k = 0; k < 2 * slots; k++) { // slot k / 2, graph parity k % 2
+      e.upload_chunk(k / 2, 0, se.staging[0], chunk.size(), SF_CHUNK_BSLZ4);
+      e.run(k / 2);
+    }
+    e.synchronize();
+    e.series[0].lab->set_next_frame(se.first_frame, e.group);
+    e.synchronize();
   }
 
   int submit(int id, const void *chunk, size_t nbytes, int algorithm, int64_t timeout_us) {
