@@ -205,9 +205,17 @@ def load_synth():
     return mod
 
 
-def make_pool(n: int, dtype=np.uint16):
-    from concurrent.futures import ThreadPoolExecutor
+def make_pool(n: int, dtype=np.uint16, threads: bool = True):
+    """n synthetic 16M frames, made on host threads unless `threads` is
+    false. The serving replay's process makes them on one thread: in a
+    process whose frames were made on 16 threads, the replay's server saw
+    stalls of 70-100 ms that dropped frames, and kept seeing them after the
+    frames were freed; the same replay after one-thread generation dropped
+    none. What in that process's state causes it was not found."""
     series = load_synth().eiger_16m(frames=max(n, 3), dtype=dtype)
+    if not threads:
+        return [series.frame(f) for f in range(n)]
+    from concurrent.futures import ThreadPoolExecutor
     with ThreadPoolExecutor(min(16, os.cpu_count() or 1)) as ex:
         return list(ex.map(series.frame, range(n)))
 
@@ -916,8 +924,8 @@ def reference_gpu_form(frame):
 def main():
     args = parse()
     if args.serve_child:
-        print(json.dumps(serving(args.serve_seconds, args.plain_seconds, make_pool(24))),
-              flush=True)
+        pool = make_pool(24, threads=False)
+        print(json.dumps(serving(args.serve_seconds, args.plain_seconds, pool)), flush=True)
         return
     ranks = Ranks()
     try:
