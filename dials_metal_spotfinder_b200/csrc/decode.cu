@@ -583,18 +583,6 @@ DeviceChunkDecoder::~DeviceChunkDecoder() {
   }
   if (h2d_)
     cudaStreamDestroy(h2d_);
-  for (int l = 0; l < kLanes; l++) {
-    if (lanes_[l]) {
-      cudaStreamSynchronize(lanes_[l]);
-      cudaStreamDestroy(lanes_[l]);
-    }
-    if (joined_[l])
-      cudaEventDestroy(joined_[l]);
-  }
-  if (fork_)
-    cudaEventDestroy(fork_);
-  if (linear_free_)
-    cudaEventDestroy(linear_free_);
   cudaFree(d_linear_);
   cudaFree(d_err_);
 }
@@ -619,40 +607,7 @@ void DeviceChunkDecoder::prepare() {
     check(cudaEventCreateWithFlags(&T.copied, cudaEventDisableTiming), "cudaEventCreate");
     check(cudaEventCreateWithFlags(&T.freed, cudaEventDisableTiming), "cudaEventCreate");
   }
-  for (int l = 0; l < kLanes; l++) {
-    check(cudaStreamCreateWithFlags(&lanes_[l], cudaStreamNonBlocking), "cudaStreamCreate");
-    check(cudaEventCreateWithFlags(&joined_[l], cudaEventDisableTiming), "cudaEventCreate");
-  }
-  check(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "cudaEventCreate");
-  check(cudaEventCreateWithFlags(&linear_free_, cudaEventDisableTiming), "cudaEventCreate");
   check(cudaStreamCreateWithFlags(&h2d_, cudaStreamNonBlocking), "cudaStreamCreate");
-}
-
-void DeviceChunkDecoder::begin(cudaStream_t s) {
-  prepare();
-  check(cudaEventRecord(fork_, s), "cudaEventRecord");
-  for (int l = 0; l < kLanes; l++)
-    check(cudaStreamWaitEvent(lanes_[l], fork_, 0), "ordering the decode streams");
-  lane_next_ = 0;
-  in_batch_ = true;
-}
-
-void DeviceChunkDecoder::end(cudaStream_t s) {
-  if (!in_batch_)
-    return;
-  in_batch_ = false;
-  for (int l = 0; l < kLanes; l++) {
-    check(cudaEventRecord(joined_[l], lanes_[l]), "cudaEventRecord");
-    check(cudaStreamWaitEvent(s, joined_[l], 0), "ordering after the decodes");
-  }
-}
-
-cudaStream_t DeviceChunkDecoder::decode_stream(cudaStream_t s) {
-  if (!in_batch_)
-    return s;
-  const cudaStream_t d = lanes_[lane_next_];
-  lane_next_ = (lane_next_ + 1) % kLanes;
-  return d;
 }
 
 DeviceChunkDecoder::Set &DeviceChunkDecoder::next_set(size_t in_bytes) {
@@ -703,11 +658,10 @@ void DeviceChunkDecoder::reserve(size_t chunk_bytes, size_t blocks) {
 }
 
 void DeviceChunkDecoder::enqueue_raw(const void *src, size_t height, size_t row_bytes, void *dst,
-                                     size_t dst_pitch, cudaStream_t caller) {
+                                     size_t dst_pitch, cudaStream_t s) {
   const size_t bytes = height * row_bytes;
   if (bytes == 0)
     return;
-  const cudaStream_t s = decode_stream(caller);
   Set &S = next_set(round16(bytes));
   check(cudaMemcpyAsync(S.d_in, src, bytes, cudaMemcpyDefault, h2d_), "copying a frame");
   check(cudaEventRecord(S.copied, h2d_), "cudaEventRecord");
@@ -718,10 +672,10 @@ void DeviceChunkDecoder::enqueue_raw(const void *src, size_t height, size_t row_
 
 void DeviceChunkDecoder::enqueue(const uint8_t *chunk, size_t nbytes, const ChunkLayout &L,
                                  size_t height, size_t width, void *dst, size_t dst_pitch,
-                                 cudaStream_t caller) {
+                                 cudaStream_t s) {
   const size_t row_bytes = width * L.elem;
   if (L.algorithm == SF_CHUNK_RAW) {
-    enqueue_raw(chunk, height, row_bytes, dst, dst_pitch, caller);
+    enqueue_raw(chunk, height, row_bytes, dst, dst_pitch, s);
     return;
   }
   const bool bs = L.algorithm == SF_CHUNK_BSLZ4;
@@ -730,7 +684,6 @@ void DeviceChunkDecoder::enqueue(const uint8_t *chunk, size_t nbytes, const Chun
   const size_t nb = L.block_in.size();
   if (nb == 0 && L.raw_bytes == 0)
     return;
-  const cudaStream_t s = decode_stream(caller);
   Set &S = next_set(round16(nbytes) + 16);
   Table &T = next_table(std::max<size_t>(nb, 1));
   BlockDesc *t = static_cast<BlockDesc *>(T.h);
@@ -754,15 +707,12 @@ void DeviceChunkDecoder::enqueue(const uint8_t *chunk, size_t nbytes, const Chun
     // plain LZ4 with blocks beyond shared memory (bitshuffle blocks never
     // are): decoded into a linear frame, then laid out at the pitch
     grow(&d_linear_, linear_cap_, round16(frame_bytes), "cudaMalloc frame staging");
-    // one linear frame at a time, whichever stream decoded the last
-    check(cudaStreamWaitEvent(s, linear_free_, 0), "ordering the linear staging");
     const unsigned grid = static_cast<unsigned>(std::max<size_t>(
         1, std::min<size_t>((nb + kDecodeWarps - 1) / kDecodeWarps,
                             static_cast<size_t>(device_sm_count()) * 16)));
     decode_linear<<<grid, kDecodeWarps * 32, 0, s>>>(S.d_in, tbl, n32, d_linear_, d_err_);
     check(cudaGetLastError(), "launching the chunk decoder");
     repitch(d_linear_, height, row_bytes, dst, dst_pitch, s);
-    check(cudaEventRecord(linear_free_, s), "cudaEventRecord");
     check(cudaEventRecord(S.freed, s), "cudaEventRecord");
     check(cudaEventRecord(T.freed, s), "cudaEventRecord");
     return;

@@ -65,13 +65,6 @@ public:
   // Allocates every staging set for chunks up to `chunk_bytes` with up to
   // `blocks` LZ4 blocks, so later calls allocate nothing.
   void reserve(size_t chunk_bytes, size_t blocks);
-  // Between begin(s) and end(s), the frames enqueued for stream s are
-  // decoded on kLanes streams of the decoder's own in turn, all after the
-  // work on s before begin(); end() makes s wait for all of them. So the
-  // decodes of a batch of chunks overlap one another (each launch's last
-  // wave with the next launch) instead of running one after another.
-  void begin(cudaStream_t s);
-  void end(cudaStream_t s);
   // Whether a block failed since the last call (synchronises the device).
   bool take_error();
   // The device flag itself (nonzero after a failed block), allocated and
@@ -80,7 +73,6 @@ public:
 
   static constexpr int kSets = 3;    // device staging buffers for chunks
   static constexpr int kTables = 32; // block tables, so the host rarely waits
-  static constexpr int kLanes = 2;   // decode streams within begin() .. end()
 
 private:
   // A chunk's (or raw frame's) bytes on the device. Ordered on the device
@@ -110,13 +102,6 @@ private:
   Table tables_[kTables];
   int next_ = 0, next_table_ = 0;
   cudaStream_t h2d_ = nullptr;
-  cudaStream_t lanes_[kLanes] = {};
-  cudaEvent_t fork_ = nullptr, joined_[kLanes] = {};
-  cudaEvent_t linear_free_ = nullptr; // the last frame through d_linear_ is laid out
-  int lane_next_ = 0;
-  bool in_batch_ = false;
-  // the stream a frame enqueued for s decodes on
-  cudaStream_t decode_stream(cudaStream_t s);
   uint8_t *d_linear_ = nullptr; // a frame decoded from blocks beyond shared memory
   size_t linear_cap_ = 0;
   int *d_err_ = nullptr;

@@ -431,25 +431,11 @@ struct Engine {
       parse(0);
     }
     check(cudaStreamWaitEvent(copy, consumed[slot], 0), "ordering after the last run");
-    // the decodes overlap one another on the decoder's streams and join the
-    // copy stream before the upload is marked done
-    struct Batch {
-      DeviceChunkDecoder &d;
-      cudaStream_t s;
-      ~Batch() {
-        try {
-          d.end(s); // on an early exit; a no-op after the end() below
-        } catch (...) {
-        }
-      }
-    } batch{decoder, copy};
-    decoder.begin(copy);
     for (size_t k = 0; k < n; k++) {
       const ThresholdPlan::Shape &sh = plan->shape(frame_of(k));
       decoder.enqueue(static_cast<const uint8_t *>(chunks[k]), nbytes[k], layouts[k], sh.height,
                       sh.width, plan->frame_origin(slot, frame_of(k)), plan->pitch() * eb, copy);
     }
-    decoder.end(copy);
     check(cudaEventRecord(uploaded[slot], copy), "cudaEventRecord");
   }
 
