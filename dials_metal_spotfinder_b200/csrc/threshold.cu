@@ -20,7 +20,7 @@
 //   - vertical 11-row running sums of the count+sum of pixels that are valid
 //     and not kept by the erode, from rows r-5 and r-16;
 //   - at row r-10, for the pixels that are candidates (value > 0 and kept
-//     by the erode), compacted one per lane, the 11 x 11 window as the sum
+//     by the erode), taken one per lane, the 11 x 11 window as the sum
 //     of 11 columns' vertical sums from shared memory, the Poisson test,
 //     and the emit of a SignalPixel into a staging pool.
 // Every window is the reference's window clipped to the frame: the arena
@@ -336,9 +336,9 @@ __device__ __forceinline__ int back_slot(int slot, int back) {
   return s < 0 ? s + kRingRows : s;
 }
 
-// Warps per SM the shared memory holds: a warp's ring, the 11-row sums of
-// two rows and their candidate list (13 KB for 16-bit pixels, 25 KB for
-// 32-bit).
+// Warps per SM the registers allow: 16 for 16-bit pixels, 8 for 32-bit
+// (whose ring and 11-row sums, 24 KB a warp, also fill the shared memory;
+// 16-bit pixels take 12.1 KB a warp).
 template <typename T> constexpr int kWarpsPerSm = sizeof(T) == 2 ? 16 : 8;
 
 // The rows before a task's first are read as zeros: 16 rows, the farthest
@@ -356,8 +356,7 @@ template <typename T> struct WarpSmem {
   static constexpr uint32_t kRing = kStripCols * sizeof(T) * kRingRows;
   static constexpr uint32_t kWin = 2 * kStripCols * sizeof(A);
   static constexpr uint32_t kBars = kRingStages * sizeof(uint64_t);
-  static constexpr uint32_t kCand = 2 * kStripOut * sizeof(uint16_t);
-  static constexpr uint32_t kTotal = kRing + kWin + kBars + kCand;
+  static constexpr uint32_t kTotal = kRing + kWin + kBars;
 };
 
 template <typename T, int WPC>
@@ -375,6 +374,9 @@ __global__ void __launch_bounds__(WPC * 32, (kWarpsPerSm<T> / WPC) > 0 ? kWarpsP
 
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   __shared__ Rl sqrt_tab[64];
+  // for each 8-bit mask, the positions of its set bits in ascending order,
+  // four bits each
+  __shared__ uint32_t bit_pos[256];
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   unsigned char *at = smem_raw;
@@ -383,11 +385,18 @@ __global__ void __launch_bounds__(WPC * 32, (kWarpsPerSm<T> / WPC) > 0 ? kWarpsP
   A *win = reinterpret_cast<A *>(at + warp * Sm::kWin);
   at += WPC * Sm::kWin;
   uint64_t *bars = reinterpret_cast<uint64_t *>(at + warp * Sm::kBars);
-  at += WPC * Sm::kBars;
-  uint16_t *cand = reinterpret_cast<uint16_t *>(at + warp * Sm::kCand);
 
   for (int m = threadIdx.x; m < 64; m += blockDim.x)
     sqrt_tab[m] = sqrt_term(m, Rl(0));
+  for (int m = threadIdx.x; m < 256; m += blockDim.x) {
+    uint32_t v = 0, n = 0;
+    for (int k = 0; k < 8; k++)
+      if ((m >> k) & 1) {
+        v |= static_cast<uint32_t>(k) << (4 * n);
+        n++;
+      }
+    bit_pos[m] = v;
+  }
   if (lane == 0) {
     for (int s = 0; s < kRingStages; s++)
       mbar_init(&bars[s], 1);
@@ -650,9 +659,10 @@ __global__ void __launch_bounds__(WPC * 32, (kWarpsPerSm<T> / WPC) > 0 ? kWarpsP
       // ---- Poisson test and emit at rows c = r-10 and c+1 ---------------
       if (flags & 4u) {
         // The 11-row sums of both rows, for the candidates' 11-column
-        // windows; then the candidates of both rows compacted one per lane
+        // windows; then the candidates of both rows taken one per lane
         // (row c's first, each row's in column order), so that each pays
-        // for one division and one square root.
+        // for one division and one square root: a prefix count over the
+        // lanes, and each lane finds its candidate by itself.
         if constexpr (sizeof(A) == 4) {
           uint4 *w0 = reinterpret_cast<uint4 *>(win + 8 * lane);
           uint4 *w1 = reinterpret_cast<uint4 *>(win + kStripCols + 8 * lane);
@@ -677,20 +687,8 @@ __global__ void __launch_bounds__(WPC * 32, (kWarpsPerSm<T> / WPC) > 0 ? kWarpsP
         }
         const uint32_t tot = __shfl_sync(kFull, incl, 31);
         const uint32_t totA = tot & 0xffffu, total = totA + (tot >> 16);
-        {
-          uint32_t ia = (incl & 0xffffu) - cntA, ib = totA + (incl >> 16) - cntB;
-          uint32_t left = csA;
-          while (left) {
-            cand[ia++] = static_cast<uint16_t>(8 * lane + __ffs(left) - 1);
-            left &= left - 1;
-          }
-          left = csB;
-          while (left) {
-            cand[ib++] = static_cast<uint16_t>(0x100u | (8 * lane + __ffs(left) - 1));
-            left &= left - 1;
-          }
-        }
-        __syncwarp();
+        const uint32_t excl = incl - (cntA | (cntB << 16));
+        const uint32_t posA = bit_pos[csA], posB = bit_pos[csB];
 
         // Room for both rows' candidates in one chunk, so each tile's
         // records are contiguous whatever the rounds below find.
@@ -715,11 +713,30 @@ __global__ void __launch_bounds__(WPC * 32, (kWarpsPerSm<T> / WPC) > 0 ? kWarpsP
         uint32_t foundA = 0, foundB = 0;
         for (uint32_t base = 0; base < total; base += 32) {
           const uint32_t i = base + lane;
+          // Candidate i (row c's in column order, then row c+1's): the lane
+          // L holding it is the first whose inclusive count for the row
+          // exceeds its rank t in the row, found by a binary search over
+          // the lanes' counts; then the (t - exclusive count)-th set bit of
+          // L's mask.
+          const bool rowB = i >= totA;
+          const uint32_t t = rowB ? i - totA : i;
+          const uint32_t sh = rowB ? 16u : 0u;
+          uint32_t L = 0;
+#pragma unroll
+          for (uint32_t step = 16; step > 0; step >>= 1) {
+            const uint32_t v = __shfl_sync(kFull, incl, static_cast<int>(L + step - 1));
+            if (((v >> sh) & 0xffffu) <= t)
+              L += step;
+          }
+          const uint32_t exL = __shfl_sync(kFull, excl, static_cast<int>(L));
+          const uint32_t pA = __shfl_sync(kFull, posA, static_cast<int>(L));
+          const uint32_t pB = __shfl_sync(kFull, posB, static_cast<int>(L));
+          const uint32_t pL = rowB ? pB : pA;
           bool sig = false;
           SignalPixel px;
           if (i < total) {
-            const uint32_t e = cand[i];
-            const uint32_t rowB = e >> 8, col = e & 0xffu; // an output column
+            const uint32_t j = t - ((exL >> sh) & 0xffffu);
+            const uint32_t col = 8 * L + ((pL >> (4 * j)) & 0xfu); // an output column
             const T *prow = row_at(back_slot(slot, rowB ? 9 : 10));
             const A *w = win + (rowB ? kStripCols : 0);
             const uint32_t pv = prow[col];
