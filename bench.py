@@ -64,7 +64,7 @@ def parse():
     # ten frames here): a reflection present at both ends of a short cycle
     # would be joined across the wrap into a streak that never closes.
     ap.add_argument("--pool", type=int, default=32, help="distinct synthetic frames")
-    ap.add_argument("--e2e-steps", type=int, default=8)
+    ap.add_argument("--e2e-steps", type=int, default=16)
     ap.add_argument("--cpu-frames", type=int, default=8)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=60.0,

@@ -637,6 +637,8 @@ int sf_server_set_pixel_mask(sf_server *server, int series, const uint8_t *mask)
     if (se.frames_done || !se.queue.empty() || !se.inflight.empty() || !se.eng)
       throw std::invalid_argument("set a series' pixel mask before its first frame");
     se.eng->set_pixel_mask(0, mask);
+    // a new mask drops the series' graphs: warm them again before frames come
+    reinterpret_cast<Server *>(server)->warm_up(se);
     return 0;
   });
 }
