@@ -5,8 +5,8 @@
 // Decomposition. A task is one strip of 256 buffer columns (232 output
 // columns plus halo) by one segment of output rows of one frame. A warp owns
 // a task at a time and walks down it row by row; warps never talk to each
-// other. Each warp has a ring of 24 rows of its strip in shared memory, fed
-// 4 rows at a time by TMA (one elected lane issues, an mbarrier per stage).
+// other. Each warp has a ring of 20 rows of its strip in shared memory, fed
+// 2 rows at a time by TMA (one elected lane issues, an mbarrier per stage).
 //
 // Per input row r entering at the bottom of the ring, each lane (8 columns)
 // updates, all in registers:
