@@ -144,26 +144,32 @@ __device__ __forceinline__ uint32_t uf_root(const uint32_t *parent, uint32_t x) 
 }
 
 // Union-find on positions. Parents only ever point to lower positions.
-__device__ __forceinline__ uint32_t uf_find(uint32_t *parent, uint32_t x) {
-  volatile uint32_t *p = parent;
-  while (true) {
-    const uint32_t px = p[x];
-    if (px == x)
-      return x;
+// Path halving: each step reads a parent and a grandparent, points the node
+// at the grandparent (still an ancestor, still lower) and moves there, so a
+// step covers two levels; a grandparent equal to its parent is the root.
+// Returns the root of x, given x's parent px already read.
+__device__ __forceinline__ uint32_t uf_find_from(volatile uint32_t *p, uint32_t x, uint32_t px) {
+  while (px != x) {
     const uint32_t gp = p[px];
-    if (gp != px)
-      p[x] = gp; // path halving: still an ancestor, still lower
-    x = px;
+    if (gp == px)
+      return px;
+    p[x] = gp;
+    x = gp;
+    px = p[x];
   }
+  return x;
 }
 
 // Joins the trees of a and b; returns the merged tree's root as it was at
 // the link (an ancestor of both from then on), so a caller uniting one
 // element with several others can pass it back as `a`.
 __device__ __forceinline__ uint32_t uf_unite(uint32_t *parent, uint32_t a, uint32_t b) {
+  volatile uint32_t *p = parent;
   while (true) {
-    a = uf_find(parent, a);
-    b = uf_find(parent, b);
+    // both parents' reads in flight before either walk
+    const uint32_t pa = p[a], pb = p[b];
+    a = uf_find_from(p, a, pa);
+    b = uf_find_from(p, b, pb);
     if (a == b)
       return a;
     if (a < b) {
