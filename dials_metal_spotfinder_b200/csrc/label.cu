@@ -396,12 +396,19 @@ __global__ void __launch_bounds__(kThreads) lab_gather(LabArgs a) {
 
 // First position (relative to the list at s0) whose index is at least t,
 // or count, given the block table's entry p for t (loaded by the caller, so
-// that independent lookups overlap).
+// that independent lookups overlap); *iq gets that position's index (not
+// set at count), which the caller's next step needs.
 __device__ __forceinline__ uint64_t first_at_least(const LabArgs &a, uint32_t p, uint64_t s0,
-                                                   uint64_t count, uint32_t t) {
+                                                   uint64_t count, uint32_t t, uint32_t *iq) {
   uint64_t q = p == kNone ? count : p;
-  while (q < count && a.ix[s0 + q] < t)
+  while (q < count) {
+    const uint32_t v = a.ix[s0 + q];
+    if (v >= t) {
+      *iq = v;
+      break;
+    }
     q++;
+  }
   return q;
 }
 
@@ -411,16 +418,23 @@ __device__ __forceinline__ uint64_t first_at_least(const LabArgs &a, uint32_t p,
 // at or past lo: the run holding that pixel, then the later run starts,
 // found in the run-start bitmap; returns the merged root.
 __device__ __forceinline__ uint32_t unite_overlaps(const LabArgs &a, uint32_t ra, uint64_t q,
-                                                   uint64_t s0, uint64_t count, uint32_t hi) {
-  if (q >= count)
+                                                   uint32_t iq, uint64_t s0, uint64_t count,
+                                                   uint32_t hi) {
+  if (q >= count || iq > hi) // iq: the index at q
     return ra;
   uint64_t p = s0 + q;
   const uint64_t end = s0 + count;
-  if (a.ix[p] > hi)
-    return ra;
+  // the run-start word of the next position, read before the union so that
+  // the two reads overlap; `wp` is a position of the word held in `word`
+  uint64_t wp = p + 1;
+  uint32_t word = wp < end ? a.run_starts[wp >> 5] : 0u;
   ra = uf_unite(a.par, ra, static_cast<uint32_t>(p));
   for (p++; p < end;) {
-    const uint32_t w = a.run_starts[p >> 5] & (0xffffffffu << (p & 31));
+    if ((p >> 5) != (wp >> 5)) {
+      wp = p;
+      word = a.run_starts[p >> 5];
+    }
+    const uint32_t w = word & (0xffffffffu << (p & 31));
     if (!w) {
       // the rest of the chunk continues the run; the next start is after it
       const uint64_t lastp = p | 31;
@@ -495,17 +509,18 @@ __global__ void __launch_bounds__(kThreads) lab_link(LabArgs a) {
     // both lookups' first loads before either walk
     const uint32_t tu = up ? table_of(a, s, first_batch_seg)[(idx - W) >> kBlockShift] : kNone;
     const uint32_t tp = prev ? table_of(a, s - 1, first_batch_seg)[idx >> kBlockShift] : kNone;
-    const uint64_t qu = up ? first_at_least(a, tu, s0, end - s0, idx - W) : end - s0;
+    uint32_t iu = 0, ip = 0;
+    const uint64_t qu = up ? first_at_least(a, tu, s0, end - s0, idx - W, &iu) : end - s0;
     uint64_t ps0 = 0, pcount = 0, qp = 0;
     if (prev) {
       ps0 = seg_start[s - 1];
       pcount = seg_count[s - 1];
-      qp = first_at_least(a, tp, ps0, pcount, idx);
+      qp = first_at_least(a, tp, ps0, pcount, idx, &ip);
     }
     if (up)
-      ra = unite_overlaps(a, ra, qu, s0, end - s0, last - W);
+      ra = unite_overlaps(a, ra, qu, iu, s0, end - s0, last - W);
     if (prev)
-      unite_overlaps(a, ra, qp, ps0, pcount, last);
+      unite_overlaps(a, ra, qp, ip, ps0, pcount, last);
   }
 }
 
