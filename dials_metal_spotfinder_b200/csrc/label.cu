@@ -956,6 +956,70 @@ __device__ void order_members(const WarpBuffers &b, uint32_t n, int lane) {
     move_runs(b, n, lane);
     return;
   }
+  if (runs <= 64) {
+    // Two runs per lane, run lane in A and run lane + 32 in B: the keys
+    // chunk << 6 | run (while every position is below 2^30, so that no key
+    // reaches the empty slots' all-ones) sorted as 64
+    // elements, element lane in A and lane + 32 in B, by the same bitonic
+    // network; the pairs at distance 32 meet within a lane.
+    const bool hb = static_cast<uint32_t>(lane) + 32 < runs;
+    const uint32_t s0a = b.ix[lane]; // runs > 32: lanes 0-31 all hold a run
+    const uint32_t s1a = b.ix[lane + 1];
+    const uint32_t s0b = hb ? b.ix[lane + 32] : 0u;
+    const uint32_t s1b = static_cast<uint32_t>(lane) + 33 < runs ? b.ix[lane + 33] : n;
+    const uint32_t ga = b.g[s0a], gb = hb ? b.g[s0b] : 0u;
+    if (!__any_sync(kFull, ((ga | gb) & 0xc0000000u) != 0)) {
+      const uint32_t lena = s1a - s0a, lenb = hb ? s1b - s0b : 0u;
+      uint32_t ka = ((ga & ~31u) << 1) | static_cast<uint32_t>(lane);
+      uint32_t kb = hb ? ((gb & ~31u) << 1) | static_cast<uint32_t>(lane + 32) : 0xffffffffu;
+#pragma unroll
+      for (int k = 2; k <= 64; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+          if (j == 32) { // k == 64: ascending, A the lower element
+            const uint32_t lo = min(ka, kb), hi = max(ka, kb);
+            ka = lo;
+            kb = hi;
+          } else {
+            const uint32_t oa = __shfl_xor_sync(kFull, ka, j);
+            const uint32_t ob = __shfl_xor_sync(kFull, kb, j);
+            const bool lower = (lane & j) == 0;
+            const bool asc_a = (lane & k) == 0, asc_b = ((lane + 32) & k) == 0;
+            ka = lower == asc_a ? min(ka, oa) : max(ka, oa);
+            kb = lower == asc_b ? min(kb, ob) : max(kb, ob);
+          }
+        }
+      }
+      // lane q holds ranks q (A) and q + 32 (B, a run while q + 32 < runs)
+      const bool rb = static_cast<uint32_t>(lane) + 32 < runs;
+      const uint32_t run_a = ka & 63u, run_b = kb & 63u;
+      auto of_run = [&](uint32_t va, uint32_t vb, uint32_t r) {
+        const uint32_t xa = __shfl_sync(kFull, va, static_cast<int>(r & 31u));
+        const uint32_t xb = __shfl_sync(kFull, vb, static_cast<int>(r & 31u));
+        return r < 32 ? xa : xb;
+      };
+      const uint32_t len_ra = of_run(lena, lenb, run_a), s0_ra = of_run(s0a, s0b, run_a);
+      const uint32_t len_rb = of_run(lena, lenb, run_b), s0_rb = of_run(s0a, s0b, run_b);
+      uint32_t inca = len_ra, incb = rb ? len_rb : 0u;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t va = __shfl_up_sync(kFull, inca, d);
+        const uint32_t vb = __shfl_up_sync(kFull, incb, d);
+        if (lane >= d) {
+          inca += va;
+          incb += vb;
+        }
+      }
+      const uint32_t half = __shfl_sync(kFull, inca, 31); // ranks 0-31's lengths
+      __syncwarp(); // every lane has read its starts before any is overwritten
+      b.ix[run_a] = s0_ra | ((inca - len_ra) << 16); // start and place, below kCompCap
+      if (rb)
+        b.ix[run_b] = s0_rb | ((half + incb - len_rb) << 16);
+      __syncwarp();
+      move_runs(b, n, lane);
+      return;
+    }
+  }
   for (uint32_t j = lane; j < runs; j += 32)
     b.val[j] = b.g[b.ix[j]] >> 5;
   __syncwarp();
