@@ -395,21 +395,40 @@ __global__ void __launch_bounds__(kThreads) lab_gather(LabArgs a) {
 }
 
 // First position (relative to the list at s0) whose index is at least t,
-// or count, given the block table's entry p for t (loaded by the caller, so
-// that independent lookups overlap); *iq gets that position's index (not
-// set at count), which the caller's next step needs.
-__device__ __forceinline__ uint64_t first_at_least(const LabArgs &a, uint32_t p, uint64_t s0,
-                                                   uint64_t count, uint32_t t, uint32_t *iq) {
-  uint64_t q = p == kNone ? count : p;
-  while (q < count) {
-    const uint32_t v = a.ix[s0 + q];
-    if (v >= t) {
-      *iq = v;
-      break;
-    }
-    q++;
+// or count, given the block table's entries p for t's block and p1 for the
+// next block (loaded by the caller, so that independent lookups overlap);
+// *iq gets that position's index (not set at count), which the caller's
+// next step needs. Indices rise by at least one a position, so position
+// p + (t mod 64) holds an index of at least t, and p1 one above t's block:
+// the answer lies in [p, min(p + t mod 64, p1)]. When that first bound
+// holds t itself (a dense stretch: every index from the block's start is
+// present) it is the answer; otherwise a binary search of the range.
+__device__ __forceinline__ uint64_t first_at_least(const LabArgs &a, uint32_t p, uint32_t p1,
+                                                   uint64_t s0, uint64_t count, uint32_t t,
+                                                   uint32_t *iq) {
+  if (p == kNone)
+    return count;
+  uint64_t lo = p;
+  uint64_t hi = min(lo + (t & ((1u << kBlockShift) - 1u)), count);
+  if (p1 != kNone)
+    hi = min(hi, static_cast<uint64_t>(p1));
+  if (hi < count) {
+    const uint32_t v = a.ix[s0 + hi];
+    *iq = v;
+    if (v == t)
+      return hi;
   }
-  return q;
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    const uint32_t v = a.ix[s0 + mid];
+    if (v >= t) {
+      hi = mid;
+      *iq = v;
+    } else {
+      lo = mid + 1;
+    }
+  }
+  return hi;
 }
 
 // Unites the tree of `ra` (the run whose first pixel is g, or an ancestor)
@@ -507,15 +526,19 @@ __global__ void __launch_bounds__(kThreads) lab_link(LabArgs a) {
     const bool up = idx >= W;
     const bool prev = !a.two_d && s > 0 && seg_z[s - 1] + 1 == seg_z[s];
     // both lookups' first loads before either walk
-    const uint32_t tu = up ? table_of(a, s, first_batch_seg)[(idx - W) >> kBlockShift] : kNone;
-    const uint32_t tp = prev ? table_of(a, s - 1, first_batch_seg)[idx >> kBlockShift] : kNone;
+    const uint32_t *tabu = up ? table_of(a, s, first_batch_seg) + ((idx - W) >> kBlockShift)
+                              : nullptr;
+    const uint32_t *tabp = prev ? table_of(a, s - 1, first_batch_seg) + (idx >> kBlockShift)
+                                : nullptr;
+    const uint32_t tu = up ? tabu[0] : kNone, tu1 = up ? tabu[1] : kNone;
+    const uint32_t tp = prev ? tabp[0] : kNone, tp1 = prev ? tabp[1] : kNone;
     uint32_t iu = 0, ip = 0;
-    const uint64_t qu = up ? first_at_least(a, tu, s0, end - s0, idx - W, &iu) : end - s0;
+    const uint64_t qu = up ? first_at_least(a, tu, tu1, s0, end - s0, idx - W, &iu) : end - s0;
     uint64_t ps0 = 0, pcount = 0, qp = 0;
     if (prev) {
       ps0 = seg_start[s - 1];
       pcount = seg_count[s - 1];
-      qp = first_at_least(a, tp, ps0, pcount, idx, &ip);
+      qp = first_at_least(a, tp, tp1, ps0, pcount, idx, &ip);
     }
     if (up)
       ra = unite_overlaps(a, ra, qu, iu, s0, end - s0, last - W);
