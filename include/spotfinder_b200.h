@@ -408,7 +408,9 @@ SF_API int sf_server_create(const sf_server_config *config, sf_server **out);
 SF_API void sf_server_destroy(sf_server *server);
 /* Admits a series of height x width frames of elem_bytes (2 or 4) pixels,
  * grouped with `options`, numbered from first_frame. -2 if its device memory
- * does not fit in what is left of the budget (retry after a close). */
+ * does not fit in what is left of the budget (retry after a close). Before
+ * returning, an empty frame goes through every slot, so that the series'
+ * first frames do not load kernels or instantiate graphs. */
 SF_API int sf_server_open(sf_server *server, size_t height, size_t width, int elem_bytes,
                           const sf_group_options *options, int64_t first_frame, int *series);
 /* The series' pixel mask (height x width bytes, nonzero = masked), as
