@@ -150,7 +150,7 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
 }
 
 // A 2D tiled TMA load of one box into shared memory, completing on `bar`.
-// No multicast: the source is always this GPU's own memory.
+// Each load fills only the issuing CTA's shared memory, from this GPU's own memory.
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map,
                                             uint64_t *bar, int32_t x,
                                             int32_t y) {
