@@ -1113,18 +1113,46 @@ __device__ void move_runs(const WarpBuffers &b, uint32_t n, int lane) {
 
 // Loads (ordering if asked) a component's members and their pixels into the
 // warp's buffers.
+template <uint32_t kU>
 __device__ void load_members(const LabArgs &a, uint32_t *m, uint32_t n, bool sort,
                              const WarpBuffers &b, int lane) {
-  for (uint32_t k = lane; k < n; k += 32)
-    b.g[k] = m[k];
+  // kU members a lane at a time, every load issued before the first store,
+  // so that a large component's reads overlap instead of following one
+  // another (the small components' launch takes one: its 64 registers are
+  // spoken for).
+  for (uint32_t k0 = lane; k0 < n; k0 += 32 * kU) {
+    uint32_t v[kU];
+#pragma unroll
+    for (uint32_t u = 0; u < kU; u++)
+      v[u] = k0 + 32 * u < n ? m[k0 + 32 * u] : 0u;
+#pragma unroll
+    for (uint32_t u = 0; u < kU; u++)
+      if (k0 + 32 * u < n)
+        b.g[k0 + 32 * u] = v[u];
+  }
   __syncwarp();
   if (sort)
     order_members(b, n, lane);
-  for (uint32_t k = lane; k < n; k += 32) {
-    const uint32_t g = b.g[k];
-    b.ix[k] = a.ix[g];
-    b.val[k] = a.val[g];
-    b.fr[k] = a.fr[g];
+  for (uint32_t k0 = lane; k0 < n; k0 += 32 * kU) {
+    uint32_t g[kU], ix[kU], val[kU];
+    int32_t fr[kU];
+#pragma unroll
+    for (uint32_t u = 0; u < kU; u++)
+      g[u] = k0 + 32 * u < n ? b.g[k0 + 32 * u] : 0u;
+#pragma unroll
+    for (uint32_t u = 0; u < kU; u++)
+      if (k0 + 32 * u < n) {
+        ix[u] = a.ix[g[u]];
+        val[u] = a.val[g[u]];
+        fr[u] = a.fr[g[u]];
+      }
+#pragma unroll
+    for (uint32_t u = 0; u < kU; u++)
+      if (k0 + 32 * u < n) {
+        b.ix[k0 + 32 * u] = ix[u];
+        b.val[k0 + 32 * u] = val[u];
+        b.fr[k0 + 32 * u] = fr[u];
+      }
   }
   __syncwarp();
 }
@@ -1343,7 +1371,7 @@ __global__ void __launch_bounds__(kCompWarps * 32, kAcceptBlocks<CAP>)
     Spot spot{}; // zeroed, padding included, so rows compare byte for byte
     bool ok;
     if (n <= CAP) {
-      load_members(a, m, n, true, b, lane);
+      load_members<CAP <= 256 ? 1 : 4>(a, m, n, true, b, lane);
       if (!spot_pass_warp(W, a.max_sep, b, n, lane, &spot, &ok))
         ok = spot_pass(W, a.max_sep, SharedMembers{b.ix, b.val, b.fr}, n, &spot);
       for (uint32_t k = lane; k < n; k += 32) {
