@@ -277,7 +277,13 @@ struct Server {
     se->eng->post_run = post_run_sink;
     se->eng->post_arg = se.get();
     se->eng->use_graph = use_graph;
-    warm_up(*se);
+    try {
+      warm_up(*se);
+    } catch (...) {
+      std::lock_guard<std::mutex> g(m);
+      used -= se->device_bytes; // the series is not opened
+      throw;
+    }
     ServerSeries *raw = se.get();
     {
       std::lock_guard<std::mutex> g(m);
