@@ -42,6 +42,7 @@
 // in position, so no loop depends on another thread making progress.
 
 #include <climits>
+#include <cstddef>
 
 #include "sf_label.hh"
 
@@ -1358,6 +1359,7 @@ __global__ void __launch_bounds__(kCompWarps * 32, kAcceptBlocks<CAP>)
       break;
     const uint64_t r = list == 0 ? i : listed[i];
     const uint32_t n = a.msize[r];
+    const uint64_t mp = a.mpk[r]; // read beside the size, not after it
     if (n == 0) {
       if (lane == 0 && lo == 0)
         a.pack[r] = 0;
@@ -1365,8 +1367,8 @@ __global__ void __launch_bounds__(kCompWarps * 32, kAcceptBlocks<CAP>)
     }
     if (n <= lo || n > hi)
       continue;
-    const uint32_t moff = static_cast<uint32_t>(a.mpk[r]);
-    const uint32_t sidx = static_cast<uint32_t>(a.mpk[r] >> 32);
+    const uint32_t moff = static_cast<uint32_t>(mp);
+    const uint32_t sidx = static_cast<uint32_t>(mp >> 32);
     uint32_t *m = a.members + moff;
     Spot spot{}; // zeroed, padding included, so rows compare byte for byte
     bool ok;
@@ -1422,23 +1424,27 @@ __global__ void __launch_bounds__(kThreads) lab_write(LabArgs a) {
   const uint64_t kept_base = sc->kept_total;
   const int lane = threadIdx.x & 31;
   const uint64_t gw = gtid() >> 5, nw = gstride() >> 5;
+  static_assert(offsetof(Spot, first) == 96, "Spot::first is the row's last word");
   for (uint64_t r = gw; r < closed; r += nw) {
+    // the component's three words read together, not one after another
     const uint32_t n = a.msize[r];
+    const uint64_t pk = a.pack[r], mp = a.mpk[r];
     if (n == 0)
       continue;
-    const uint64_t row = a.pack[r] & 0xffffffffu;
-    const uint64_t pix = a.pack[r] >> 32;
-    const uint32_t moff = static_cast<uint32_t>(a.mpk[r]);
-    const uint32_t sidx = static_cast<uint32_t>(a.mpk[r] >> 32);
+    const uint64_t row = pk & 0xffffffffu;
+    const uint64_t pix = pk >> 32;
+    const uint32_t moff = static_cast<uint32_t>(mp);
+    const uint32_t sidx = static_cast<uint32_t>(mp >> 32);
     if (row >= a.spot_cap || sidx >= a.spot_cap || pix + n > a.live_cap) {
       if (lane == 0)
         sc->status = kLabelSpotOverflow;
       continue;
     }
-    if (lane == 0) {
-      Spot spot = a.spot_tmp[sidx];
-      spot.first = kept_base + pix;
-      a.spots[row] = spot;
+    // the 104-byte row as 13 words, one a lane; the last is Spot::first
+    if (lane < 13) {
+      const uint64_t *src = reinterpret_cast<const uint64_t *>(a.spot_tmp + sidx);
+      uint64_t *dst = reinterpret_cast<uint64_t *>(a.spots + row);
+      dst[lane] = lane == 12 ? kept_base + pix : src[lane];
     }
     for (uint32_t k = lane; k < n; k += 32)
       a.kept[pix + k] = a.pix_tmp[moff + k];
