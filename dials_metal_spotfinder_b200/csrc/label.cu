@@ -571,9 +571,9 @@ __global__ void __launch_bounds__(kThreads) lab_flatten(LabArgs a) {
     uint32_t r = kNone;
     int32_t z = INT_MIN;
     if (g < n) {
+      z = a.fr[g]; // read before the walk, which it does not depend on
       r = uf_root(a.par, static_cast<uint32_t>(g)); // lab_link is done: no more links
       a.root[g] = r;
-      z = a.fr[g];
     }
     const uint32_t before = __shfl_up_sync(kFull, r, 1);
     const bool head = lane == 0 || before != r;
@@ -693,14 +693,19 @@ __global__ void __launch_bounds__(kThreads) lab_scatter(LabArgs a) {
   const uint64_t warps = gstride() >> 5;
   for (uint64_t base = (gtid() >> 5) * 32; base < n; base += warps * 32) {
     const uint64_t g = base + lane;
-    uint32_t r = kNone, rank = kNone;
+    uint32_t r = kNone, rank = kNone, moff = 0;
     bool open = false;
     if (g < n) {
       r = a.root[g];
       rank = a.rank_of_root[r];
       open = rank == kNone; // not finished by this batch: carried
-      if (rank != kNone && a.msize[rank] == 0)
-        rank = kNone;
+      if (rank != kNone) {
+        // the component's size and member offset read together
+        const uint32_t size = a.msize[rank];
+        moff = static_cast<uint32_t>(a.mpk[rank]);
+        if (size == 0)
+          rank = kNone;
+      }
     }
     const uint32_t ob = __ballot_sync(kFull, open);
     if (lane == 0) {
@@ -716,7 +721,7 @@ __global__ void __launch_bounds__(kThreads) lab_scatter(LabArgs a) {
     if (lane == leader)
       at = atomicAdd(&a.cursor[r], static_cast<uint32_t>(__popc(peers)));
     at = __shfl_sync(peers, at, leader) + __popc(peers & ((1u << lane) - 1u));
-    a.members[static_cast<uint32_t>(a.mpk[rank]) + at] = static_cast<uint32_t>(g);
+    a.members[moff + at] = static_cast<uint32_t>(g);
   }
 }
 
@@ -1467,11 +1472,11 @@ __global__ void __launch_bounds__(kThreads) lab_carry(LabArgs a) {
   const int lane = threadIdx.x & 31;
   const uint64_t warps = gstride() >> 5;
   for (uint64_t w = gtid() >> 5; w < nw; w += warps) {
-    const uint32_t bits = a.obits[w];
+    const uint32_t bits = a.obits[w], cnt = a.ocnt[w]; // read together
     if (!((bits >> lane) & 1u))
       continue;
     const uint64_t g = w * 32 + static_cast<uint64_t>(lane);
-    const uint32_t at = a.ocnt[w] + __popc(bits & ((1u << lane) - 1u));
+    const uint32_t at = cnt + __popc(bits & ((1u << lane) - 1u));
     const uint32_t r = a.root[g];
     a.nfr[at] = a.fr[g];
     a.nix[at] = a.ix[g];
