@@ -1,6 +1,7 @@
 """The batched engine's autotuner (include/spotfinder_b200.h, sf_tune): a
-timed search on the current device for frames per launch, warps per block
-and threshold task height, on sample frames of one shape. The result goes
+timed search on the current device for frames per launch, warps per block,
+threshold task height and threshold blocks per SM, on sample frames of one
+shape. The result goes
 to a tuner file that engines created without explicit tuning read. The
 reference chooses its own stage windows by measurement the same way
 (src/dext_gpu.cc:18-37, tests/bench_dext_gpu.cc:242-337)."""
@@ -20,8 +21,9 @@ def tune(frames, min_frames: int = 8, max_frames: int = 32, steps: int = 4,
     """Tunes the engine for the shape and type of `frames` (a sequence of
     consecutive frames, cycled into the trial batches). Returns the chosen
     frames_per_launch, warps_per_block, seg_rows (for that many frames),
-    seg_ratio, us_per_frame, candidates (configurations timed) and
-    from_cache (read from the tuner file, nothing timed)."""
+    seg_ratio, blocks_per_sm (0: as many as fit), us_per_frame, candidates
+    (configurations timed) and from_cache (read from the tuner file,
+    nothing timed)."""
     require_device()
     frames = [np.ascontiguousarray(f) for f in frames]
     if not frames:
