@@ -63,8 +63,8 @@ class Engine:
         return dict(zip(keys, list(out)))
 
     def tuning(self) -> dict:
-        """frames_per_launch, warps_per_block, seg_rows and from_cache (the
-        tuning came from the tuner file)."""
+        """frames_per_launch, warps_per_block, seg_rows, blocks_per_sm and
+        from_cache (the tuning came from the tuner file)."""
         out = TuneResult()
         raise_for(lib.sf_engine_tuning(self._h, ctypes.byref(out)), "sf_engine_tuning")
         d = out.as_dict()
